@@ -1,0 +1,270 @@
+// CPU oracle -- TEST INFRASTRUCTURE ONLY.
+//
+// Flat C entry points over the oracle so that the pytest suite, the smoke
+// check and the CPU-baseline leg of bench.py can drive it through ctypes.
+// Complex arrays are interleaved (re, im) doubles; matrices are column-major.
+// Every entry point catches exceptions and returns a negative status.
+#include <omp.h>
+
+#include <cstring>
+#include <memory>
+
+#include "tree.hpp"
+
+using namespace orc;
+
+namespace {
+thread_local std::string g_err;
+int guard(const std::exception& e) {
+  g_err = e.what();
+  return -1;
+}
+void putMat(const Mat& m, double* out) { std::memcpy(out, m.a.data(), sizeof(cd) * m.a.size()); }
+Mat getVec(const double* in, int n) {
+  Mat v(n, 1);
+  std::memcpy(v.a.data(), in, sizeof(cd) * n);
+  return v;
+}
+struct Solver {
+  std::unique_ptr<Tree> t;
+};
+}  // namespace
+
+extern "C" {
+
+const char* or_last_error() { return g_err.c_str(); }
+void or_set_threads(int n) { omp_set_num_threads(n); }
+int or_get_threads() { return omp_get_max_threads(); }
+
+// EFIE kernel over a triangle mesh: xyz = nv x 3 vertex coordinates, tris =
+// nt x 3 one-based vertex ids (patchList format).
+void* or_efie_create(const double* xyz, int nv, const int* tris, int nt, double freq, int exact_lookup) {
+  try {
+    return new EFIE(xyz, nv, tris, nt, freq, exact_lookup != 0);
+  } catch (const std::exception& e) {
+    guard(e);
+    return nullptr;
+  }
+}
+void* or_es_create(const double* xyz, int nv, const int* tris, int nt, const int* cond) {
+  try {
+    return new Electrostatics(xyz, nv, tris, nt, cond);
+  } catch (const std::exception& e) {
+    guard(e);
+    return nullptr;
+  }
+}
+void or_kernel_destroy(void* k) { delete static_cast<Kernel*>(k); }
+int or_kernel_n(void* k) { return static_cast<Kernel*>(k)->N; }
+
+int or_kernel_matrix(void* k, const int* rows, int nr, const int* cols, int nc, double* out) {
+  try {
+    std::vector<int> r(rows, rows + nr), c(cols, cols + nc);
+    Mat m = static_cast<Kernel*>(k)->getMatrix(r, c);
+    putMat(m, out);
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+int or_kernel_locations(void* k, double* xyz) {
+  std::vector<V3> loc;
+  static_cast<Kernel*>(k)->locations(loc);
+  for (size_t i = 0; i < loc.size(); ++i)
+    for (int q = 0; q < 3; ++q) xyz[3 * i + q] = loc[i][q];
+  return 0;
+}
+
+// RWG table of the EFIE kernel: per unknown (n1, n2, t+, t-, free+, free-) and length.
+int or_efie_rwg(void* k, int* table, double* len) {
+  EFIE* e = static_cast<EFIE*>(k);
+  for (int i = 0; i < e->N; ++i) {
+    table[6 * i + 0] = e->eNodes[i].first;
+    table[6 * i + 1] = e->eNodes[i].second;
+    table[6 * i + 2] = e->ePlus[i];
+    table[6 * i + 3] = e->eMinus[i];
+    table[6 * i + 4] = e->thirdNode(e->ePlus[i], e->eNodes[i].first, e->eNodes[i].second);
+    table[6 * i + 5] = e->thirdNode(e->eMinus[i], e->eNodes[i].first, e->eNodes[i].second);
+    len[i] = e->eLen[i];
+  }
+  return 0;
+}
+
+// Reference RHS (EFIEMatrix.cpp:785-829, Einc real 3-vector).
+int or_efie_rhs_reference(void* k, const double* Einc, double* out) {
+  EFIE* e = static_cast<EFIE*>(k);
+  V3 E(Einc[0], Einc[1], Einc[2]);
+  for (int i = 0; i < e->N; ++i) {
+    cd v = e->rhsReference(E, i);
+    out[2 * i] = v.real();
+    out[2 * i + 1] = v.imag();
+  }
+  return 0;
+}
+// Plane wave travelling along khat with complex polarisation E0 (6 doubles).
+int or_efie_rhs_plane(void* k, const double* khat, const double* E0, double* out) {
+  EFIE* e = static_cast<EFIE*>(k);
+  V3 kh(khat[0], khat[1], khat[2]);
+  C3 E(cd(E0[0], E0[1]), cd(E0[2], E0[3]), cd(E0[4], E0[5]));
+  for (int i = 0; i < e->N; ++i) {
+    cd v = e->rhsPlaneWave(kh, E, i);
+    out[2 * i] = v.real();
+    out[2 * i + 1] = v.imag();
+  }
+  return 0;
+}
+
+// Dense LU solve (EFIEMatrix.cpp:831-837) for nrhs right-hand sides.
+int or_dense_solve(void* k, const double* rhs, int nrhs, double* x) {
+  try {
+    Kernel* K = static_cast<Kernel*>(k);
+    std::vector<int> all(K->N);
+    for (int i = 0; i < K->N; ++i) all[i] = i;
+    Mat A = K->getMatrix(all, all);
+    LU lu(A);
+    Mat B(K->N, nrhs);
+    std::memcpy(B.a.data(), rhs, sizeof(cd) * B.a.size());
+    Mat X = lu.solve(B);
+    putMat(X, x);
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+// ACA_only_nodes2 on global ids; returns rank or <0.  row_bases/col_bases
+// hold min(nr,nc) ints; Ac is nr x rank, Ar is rank x nc (space for min(nr,nc)).
+int or_aca(void* k, const int* rows, int nr, const int* cols, int nc, double tol, int* row_bases, int* col_bases,
+           double* Ac, double* Ar) {
+  try {
+    std::vector<int> r(rows, rows + nr), c(cols, cols + nc);
+    ACAResult res;
+    acaOnlyNodes2(*static_cast<Kernel*>(k), tol, r, c, res);
+    for (size_t i = 0; i < res.rowBases.size(); ++i) row_bases[i] = res.rowBases[i];
+    for (size_t i = 0; i < res.colBases.size(); ++i) col_bases[i] = res.colBases[i];
+    putMat(res.Ac, Ac);
+    putMat(res.Ar, Ar);
+    return res.rank;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+// RRQR with partition; A is m x n; Q gets m x rank, R rank x n, perm n ints.
+int or_rrqr(const double* A, int m, int n, int tolpow1, int tolpow2, int partition, double inputPivot,
+            int fillInRank, int realMode, double* Q, double* R, int* perm, double* maxPivot, double* err) {
+  try {
+    Mat M(m, n);
+    std::memcpy(M.a.data(), A, sizeof(cd) * M.a.size());
+    RRQRResult r;
+    rrqrPartition(M, tolpow1, tolpow2, partition, inputPivot, fillInRank, realMode != 0, r);
+    putMat(r.Q, Q);
+    putMat(r.R, R);
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i)
+        if (r.P(i, j) == cd(1.0, 0.0)) perm[j] = i;
+    *maxPivot = r.maxPivot;
+    *err = rrqrError(M, r);
+    return r.rank;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+int or_lu_solve(const double* A, int n, const double* B, int nrhs, double* X) {
+  try {
+    Mat M(n, n);
+    std::memcpy(M.a.data(), A, sizeof(cd) * M.a.size());
+    Mat Bm(n, nrhs);
+    std::memcpy(Bm.a.data(), B, sizeof(cd) * Bm.a.size());
+    LU lu(M);
+    putMat(lu.solve(Bm), X);
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+// AIFMM<K>(inputsToSolverClass, K*): bbox = xmin,xmax,ymin,ymax,zmin,zmax;
+// locations = N x 3.  Builds the tree and every block (AIFMM.cpp:7-93).
+void* or_aifmm_create(void* k, const double* bbox, int leafSize, int tol_pow, int nLevelsInput, int fillin_rank,
+                      int fillin_tol, const double* locations, int realMode) {
+  try {
+    Kernel* K = static_cast<Kernel*>(k);
+    SolverInputs in;
+    in.xmin = bbox[0]; in.xmax = bbox[1];
+    in.ymin = bbox[2]; in.ymax = bbox[3];
+    in.zmin = bbox[4]; in.zmax = bbox[5];
+    in.leafSize = leafSize;
+    in.tol_pow = tol_pow;
+    in.nLevelsInput = nLevelsInput;
+    in.fillin_rank = fillin_rank;
+    in.fillin_tol = fillin_tol;
+    in.locations.resize(K->N);
+    for (int i = 0; i < K->N; ++i)
+      in.locations[i] = V3(locations[3 * i], locations[3 * i + 1], locations[3 * i + 2]);
+    auto* s = new Solver;
+    s->t.reset(new Tree(in, K, realMode != 0));
+    s->t->build();
+    return s;
+  } catch (const std::exception& e) {
+    guard(e);
+    return nullptr;
+  }
+}
+void or_aifmm_destroy(void* s) { delete static_cast<Solver*>(s); }
+
+int or_aifmm_factorize(void* s) {
+  try {
+    static_cast<Solver*>(s)->t->factorize();
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+int or_aifmm_solve(void* s, const double* rhs, double* x) {
+  try {
+    Tree* t = static_cast<Solver*>(s)->t.get();
+    Mat b = getVec(rhs, t->N), xs;
+    t->solve(b, xs);
+    putMat(xs, x);
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
+
+// info[0..7]: nLevels, startLevel, avgLeafSize, avgMultipoles, maxRank,
+// nRRQR, nCompressP2P, nCompressP2L; times[0..2]: assemble, factor, solve;
+// mem[0..1]: findMemory, findMemoryAfterFactorize (GB of doubles).
+int or_aifmm_info(void* s, long* info, double* times, double* mem) {
+  Tree* t = static_cast<Solver*>(s)->t.get();
+  info[0] = t->nLevels;
+  info[1] = t->startLevel;
+  info[2] = t->getAvgLeafSize();
+  info[3] = t->getAvgMultipoles();
+  info[4] = t->maxRank();
+  info[5] = t->stats.nRRQR;
+  info[6] = t->stats.nCompressP2P;
+  info[7] = t->stats.nCompressP2L;
+  times[0] = t->stats.tAssemble;
+  times[1] = t->stats.tFactor;
+  times[2] = t->stats.tSolve;
+  if (mem) {
+    mem[0] = t->findMemory();
+    mem[1] = t->findMemoryAfterFactorize();
+  }
+  return 0;
+}
+
+// Leaf boxes: for each leaf box its charge count; used to compare trees.
+int or_aifmm_leaf_counts(void* s, int* counts) {
+  Tree* t = static_cast<Solver*>(s)->t.get();
+  int n = t->nBoxesPerLevel[t->nLevels];
+  for (int k = 0; k < n; ++k) counts[k] = (int)t->tree[t->nLevels][k].chargeLocations.size();
+  return n;
+}
+
+}  // extern "C"
