@@ -1,0 +1,364 @@
+#!/usr/bin/env python
+"""Benchmark of the AIFMM factor+solve on B200.
+
+One step = factorize + solve of the assembled EFIE operator (the checkpointed
+assembly is restored on the device at the start of each step, inside the
+timed region).  The metric is the reference's: seconds of factor+solve at the
+stated relative residual.  Prints one JSON line (rank 0).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--config c3] [--impl reference]
+
+Under torchrun each rank runs an independent replica of the workload on its
+own GPU (one geometry does not shard: replicas only); the step time is the
+maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "factor+solve s at rel. residual 1e-6: mixed/batched/learned vs plain FP64 GPU"
+
+# Workloads; synthetic icosphere meshes, seeded plane waves.
+CONFIGS = {
+    "c1": dict(sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0,
+               desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10"),
+    "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=7, fillin_tol=9, nrhs=8, levels=0,
+               desc="EFIE PEC sphere R=0.15 m f=4 GHz, 81,920 tri, N=122,880, leaf 128, ACA 1e-7, RRQR 1e-9, "
+                    "8 plane waves"),
+    "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=7, fillin_tol=9, nrhs=8, levels=0,
+                desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-7, RRQR 1e-9, "
+                     "8 plane waves (c3 shape at 1/4 size)"),
+}
+# CPU sample for the reference arm and cpu_baseline: same tree depth as c3
+# (nLevels = 3, N / leaf = 960) at 1/16 of the unknowns.
+CPU_SAMPLE = dict(sub=4, radius=0.15, freq=1.0e9, leaf=8, tol_pow=7, fillin_tol=9, nrhs=1, levels=0)
+
+
+def plane_waves(n: int, seed: int = 4):
+    """Seeded incidence directions uniform on the sphere (theta = acos(1-2u),
+    phi = 2 pi u), alternating theta/phi polarisation."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    out = []
+    for q in range(n):
+        th = math.acos(1 - 2 * rng.random())
+        ph = 2 * math.pi * rng.random()
+        k = np.array([math.sin(th) * math.cos(ph), math.sin(th) * math.sin(ph), math.cos(th)])
+        e_th = np.array([math.cos(th) * math.cos(ph), math.cos(th) * math.sin(ph), -math.sin(th)])
+        e_ph = np.array([-math.sin(ph), math.cos(ph), 0.0])
+        out.append((k, (e_th if q % 2 == 0 else e_ph).astype(np.complex128)))
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, device: int):
+        self.device = device
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 3 + i and r[3 + i] == "Active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def max_over_ranks(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def build_workload(cfg, device: int):
+    from rcs_b200 import mesh as M
+    from rcs_b200.kernel import Context, EFIEMatrix
+    from rcs_b200.solver import AIFMM
+    ctx = Context(device)
+    m = M.icosphere(cfg["sub"], cfg["radius"])
+    K = EFIEMatrix(m, cfg["freq"], ctx=ctx)
+    waves = plane_waves(cfg["nrhs"]) if cfg["nrhs"] > 1 else [(np.array([0.0, 0, -1]), np.array([1, 0, 0j]))]
+    B = np.stack([K.planeWaveRhs(k, e) for k, e in waves], axis=1)
+    t0 = time.perf_counter()
+    S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"])
+    t_asm = time.perf_counter() - t0
+    S.checkpoint()
+    return ctx, m, K, S, B, t_asm
+
+
+def sampled_residual(K, X: np.ndarray, B: np.ndarray, nrows: int = 2048, seed: int = 1) -> float:
+    """||A x - b|| / ||b|| over a seeded sample of rows (full rows of A on the GPU)."""
+    rng = np.random.default_rng(seed)
+    rows = np.sort(rng.choice(K.N, size=min(nrows, K.N), replace=False))
+    acc = np.zeros((len(rows), X.shape[1]), dtype=np.complex128)
+    for c0 in range(0, K.N, 16384):
+        cols = np.arange(c0, min(K.N, c0 + 16384))
+        acc += K.getMatrix(rows, cols) @ X[cols]
+    r = acc - B[rows]
+    return float(np.linalg.norm(r) / np.linalg.norm(B[rows]))
+
+
+def zgemm_peak_tflops() -> float:
+    """cuBLAS complex128 GEMM throughput on this GPU (the FP64 denominator)."""
+    import torch
+    n = 4096
+    a = torch.randn(n, n, dtype=torch.complex128, device="cuda")
+    b = torch.randn(n, n, dtype=torch.complex128, device="cuda")
+    for _ in range(2):
+        a @ b
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    best = 1e30
+    for _ in range(5):
+        e0.record()
+        a @ b
+        e1.record()
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1) / 1e3)
+    return 8.0 * n ** 3 / best / 1e12
+
+
+def cpu_sample_seconds(threads: int):
+    """Oracle (the reference's CPU algorithm restated) factor+solve on the CPU
+    sample, and the same sample's algorithmic factorization flops (counted by
+    the GPU run of the identical algorithm)."""
+    import oracle
+    from rcs_b200 import mesh as M
+    oracle.set_threads(threads)
+    m = M.icosphere(CPU_SAMPLE["sub"], CPU_SAMPLE["radius"])
+    O = oracle.EFIE(m, CPU_SAMPLE["freq"])
+    b = O.rhs_plane((0, 0, -1), (1, 0, 0))
+    S = oracle.AIFMM(O, leaf_size=CPU_SAMPLE["leaf"], tol_pow=CPU_SAMPLE["tol_pow"],
+                     fillin_tol=CPU_SAMPLE["fillin_tol"], n_levels=CPU_SAMPLE["levels"])
+    t0 = time.perf_counter()
+    S.factorize()
+    S.solve(b)
+    return time.perf_counter() - t0, m
+
+
+def run_reference(args, rank, world):
+    """Reference arm: the reference's algorithm on the host CPU (the oracle
+    port; the reference itself needs Eigen 3, absent here), timed on a bounded
+    sample and scaled to the workload by algorithmic factorization flops."""
+    if rank != 0:
+        return
+    cfg = CONFIGS[args.config]
+    threads = os.cpu_count() or 1
+    # flops of the full workload and of the sample, from GPU runs of the same algorithm
+    from rcs_b200 import mesh as M
+    from rcs_b200.kernel import Context, EFIEMatrix
+    from rcs_b200.solver import AIFMM
+    ctx = Context(0)
+    flops = {}
+    for name, c in (("full", cfg), ("sample", CPU_SAMPLE)):
+        K = EFIEMatrix(M.icosphere(c["sub"], c["radius"]), c["freq"], ctx=ctx)
+        S = AIFMM(K, leaf_size=c["leaf"], tol_pow=c["tol_pow"], fillin_tol=c["fillin_tol"], n_levels=c["levels"])
+        S.factorize()
+        flops[name] = S.info()["flops_factor"]
+        S.close()
+        K.close()
+    times = []
+    for _ in range(args.warmup if args.warmup < 1 else 1):
+        cpu_sample_seconds(threads)
+    for _ in range(args.steps):
+        t, _ = cpu_sample_seconds(threads)
+        times.append(t * flops["full"] / flops["sample"])
+    v = float(np.mean(times))
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": cfg["desc"], "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
+                             "sample": f"oracle factor+solve of icosphere {CPU_SAMPLE['sub']} (N=7,680, leaf 8, "
+                                       f"same depth) scaled by factorization flops x{flops['full'] / flops['sample']:.1f}"},
+            "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--config", default=os.environ.get("AIFMM_BENCH_CONFIG", "c3"))
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, world, local = dist_env()
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        from datetime import timedelta
+        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    import torch
+    torch.cuda.set_device(local)
+    from rcs_b200.solver import launch_count, profile_gemm, profile_gemm_read
+    cfg = CONFIGS[args.config]
+    ctx, m, K, S, B, t_asm = build_workload(cfg, local)
+    N, nrhs = K.N, B.shape[1]
+    stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
+    Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(f"cuda:{local}")  # nrhs x N == column-major N x nrhs
+    Xd = torch.empty_like(Bd)
+
+    def step():
+        S.rewind()
+        S.factorize()
+        S.solve_device(Bd.data_ptr(), nrhs, Xd.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(args.steps):
+            step()
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = launch_count() - l0
+    barrier(world)
+    t_step = max_over_ranks(e0.elapsed_time(e1) / 1e3 / args.steps, world)
+    X = Xd.cpu().numpy().T
+    res = sampled_residual(K, X, B)
+    info = S.info()
+
+    # e2e: the public host API, pinned host buffers, H2D/D2H inside the step
+    Bh = torch.from_numpy(np.ascontiguousarray(B.T)).pin_memory()
+    Xh = torch.empty_like(Bh).pin_memory()
+    from rcs_b200 import _lib
+    import ctypes as C
+    barrier(world)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        S.rewind()
+        S.factorize()
+        _lib.check(_lib.lib().aifmm_solver_solve(S.h, np.ctypeslib.as_array(
+            C.cast(Bh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,)), nrhs,
+            np.ctypeslib.as_array(C.cast(Xh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))))
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+
+    # roofline of the dominant kernel (grouped complex GEMM) over one more step
+    profile_gemm(True)
+    step()
+    torch.cuda.synchronize()
+    g_ms, g_flops, g_n = profile_gemm_read()
+    profile_gemm(False)
+    peak = zgemm_peak_tflops()
+    achieved = g_flops / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0
+
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        t_s, _ = cpu_sample_seconds(threads)
+        # scale by the factorization flops of the workload vs the sample
+        from rcs_b200 import mesh as M
+        from rcs_b200.kernel import EFIEMatrix
+        from rcs_b200.solver import AIFMM
+        Ks = EFIEMatrix(M.icosphere(CPU_SAMPLE["sub"], CPU_SAMPLE["radius"]), CPU_SAMPLE["freq"], ctx=ctx)
+        Ss = AIFMM(Ks, leaf_size=CPU_SAMPLE["leaf"], tol_pow=CPU_SAMPLE["tol_pow"],
+                   fillin_tol=CPU_SAMPLE["fillin_tol"], n_levels=CPU_SAMPLE["levels"])
+        Ss.factorize()
+        scale = info["flops_factor"] / max(Ss.info()["flops_factor"], 1.0)
+        cpu = {"value": t_s * scale, "unit": "s", "cores": threads, "kind": "port",
+               "sample": f"oracle factor+solve of icosphere {CPU_SAMPLE['sub']} (N=7,680, leaf 8, same tree depth) "
+                         f"= {t_s:.2f} s, scaled by factorization flops x{scale:.1f}"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs, "path": "plain complex128 (reference control flow)",
+                       "parallelism": "replicas" if world > 1 else "single GPU",
+                       "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"},
+            "residual": res, "residual_rows_sampled": min(2048, N),
+            "assemble_s": t_asm, "factor_flops": info["flops_factor"],
+            "tree": {"levels": info["n_levels"], "avg_leaf": info["avg_leaf_size"], "avg_rank": info["avg_multipoles"],
+                     "max_rank": info["max_rank"], "rrqr": info["n_rrqr"]},
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "tensor", "kernel": "zgemm_grouped_kernel", "achieved": achieved,
+                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
+                         "peak_source": "measured cuBLAS complex128 GEMM 4096^3 on this GPU (FP64 path; "
+                                        "MEASURED_PEAKS.json has no FP64 figure)",
+                         "traffic": None, "launches_profiled": g_n},
+            "clocks": clk.summary(),
+            "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(16 * N * nrhs),
+                    "d2h_bytes_per_step": int(16 * N * nrhs)},
+            "cpu_baseline": cpu,
+        }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

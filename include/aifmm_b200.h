@@ -1,0 +1,178 @@
+/*
+ * aifmm_b200.h -- C ABI of the B200 AIFMM library (libaifmm_b200.so).
+ *
+ * The library implements the hot path of the vaishna77/RCS AIFMM direct
+ * solver on one NVIDIA B200: Green's-function matrix-entry assembly (EFIE
+ * with RWG basis functions, and piecewise-constant electrostatics), ACA
+ * skeletonisation with RRQR recompression, the level-by-level hierarchical
+ * elimination and the forward/backward solve sweeps.  The C++ drop-in
+ * classes (AIFMM<K>, FMM2DTree<K>, EFIEMatrix, ...) and the Python package
+ * are thin callers of these entry points.
+ *
+ * Conventions
+ *   - Every function returns an int status: AIFMM_OK (0) or a negative
+ *     AIFMM_E* code; aifmm_last_error() describes the last failure of the
+ *     calling thread.
+ *   - Complex numbers are interleaved (re, im) doubles; matrices are
+ *     column-major with a leading dimension ld >= rows.
+ *   - Unknown ids are zero-based; triangle vertex ids are ONE-based, as in the
+ *     reference's patchList files (src/EFIEMatrix.cpp:72-95).
+ *   - Host pointers unless the name ends in _device.  A context owns all
+ *     device memory and one CUDA stream; calls on one context must not
+ *     overlap (they are not re-entrant).
+ */
+#ifndef AIFMM_B200_H
+#define AIFMM_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define AIFMM_OK 0
+#define AIFMM_EINVAL (-1)    /* bad argument */
+#define AIFMM_ECUDA (-2)     /* CUDA runtime error */
+#define AIFMM_ENOMEM (-3)    /* device or host allocation failed */
+#define AIFMM_ETIMEOUT (-4)  /* a bounded device wait gave up */
+#define AIFMM_ESTATE (-5)    /* call out of order (e.g. solve before factorize) */
+#define AIFMM_ESINGULAR (-6) /* exactly singular pivot met */
+#define AIFMM_ENOTIMPL (-7)  /* feature not available in this build */
+#define AIFMM_EOVERFLOW (-8) /* a workspace bound was exceeded */
+
+typedef struct aifmm_ctx aifmm_ctx;
+typedef struct aifmm_kernel aifmm_kernel;
+typedef struct aifmm_solver aifmm_solver;
+
+/* ---- context ------------------------------------------------------------ */
+/* Message of the last failed call on the calling thread. */
+const char* aifmm_last_error(void);
+int aifmm_ctx_create(int device, aifmm_ctx** out);
+int aifmm_ctx_destroy(aifmm_ctx* ctx);
+int aifmm_ctx_synchronize(aifmm_ctx* ctx);
+/* The context's CUDA stream (a cudaStream_t), for callers that time or
+ * overlap work on it. */
+int aifmm_ctx_stream(aifmm_ctx* ctx, void** stream);
+
+/* ---- matrix-entry kernels ------------------------------------------------ */
+/* EFIE kernel over a flat-triangle mesh: replaces
+ * EFIEMatrix::EFIEMatrix(inputsToKernelClass) (src/EFIEMatrix.cpp:5-20) --
+ * the RWG unknowns are numbered in the reference's std::map order of
+ * (min node, max node) edge keys; "+" triangle = first patch in file order.
+ * nodes: n_nodes x 3; tris: n_tris x 3 one-based ids; freq in Hz (the
+ * reference hard-codes 1e7, include/includes.hpp:58). */
+int aifmm_kernel_create_efie(aifmm_ctx* ctx, const double* nodes, int n_nodes, const int* tris, int n_tris,
+                             double freq, aifmm_kernel** out);
+/* Electrostatics kernel (collocation at centroids, piecewise-constant
+ * charge): replaces ElectrostaticsMatrix::ElectrostaticsMatrix
+ * (src/ElectrostaticsMatrix.cpp:48-52).  cond may be NULL (all 1). */
+int aifmm_kernel_create_es(aifmm_ctx* ctx, const double* nodes, int n_nodes, const int* tris, const int* cond,
+                           int n_tris, aifmm_kernel** out);
+int aifmm_kernel_destroy(aifmm_kernel* k);
+/* EFIE only: 0 (default) keeps the reference's projection of the test point
+ * onto the source triangle's normal plane through the ORIGIN
+ * (findProjectionOnTriangle, src/EFIEMatrix.cpp:457-476); 1 projects onto the
+ * triangle's own plane, which makes the RCS of a sphere match the Mie series.
+ * No counterpart in the reference beyond that one function. */
+int aifmm_kernel_set_plane_projection(aifmm_kernel* k, int on);
+/* kernel::N -- number of unknowns (EFIEMatrix::getSizeOfMatrix, :97-99). */
+int aifmm_kernel_size(const aifmm_kernel* k, int* n);
+/* Unknown locations, n x 3: RWG-edge midpoints (EFIE; as the driver builds
+ * them, test/sphere.cpp:143-152) or triangle centroids (electrostatics,
+ * ElectrostaticsMatrix::getCentroids, :82-88). */
+int aifmm_kernel_locations(const aifmm_kernel* k, double* xyz);
+/* Dense block of entries K(rows[a], cols[b]) into out (nr x nc, leading
+ * dimension ld): replaces kernel::getMatrix(row_indices, col_indices)
+ * (src/kernel.cpp:49-61), and with nr==1 / nc==1 kernel::getRow / getCol
+ * (:11-29).  precision 0 = complex128 output, 1 = complex64 output (out is
+ * then interleaved floats). */
+int aifmm_kernel_matrix(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc, int precision,
+                        void* out, int ld);
+/* Same with device pointers, asynchronous on the context stream. */
+int aifmm_kernel_matrix_device(aifmm_kernel* k, const int* rows_device, int nr, const int* cols_device, int nc,
+                               int precision, void* out_device, int ld);
+/* EFIE right-hand side exactly as EFIEMatrix::getRhs (src/EFIEMatrix.cpp:785-829),
+ * including its phase quirk (exp(i z) for the default incidence). */
+int aifmm_kernel_rhs_reference(aifmm_kernel* k, const double einc[3], double* out);
+/* Physical plane wave E0 exp(-i kappa khat.r), khat = propagation direction,
+ * e0 = complex polarisation (6 doubles), sampled at the triangle centroids. */
+int aifmm_kernel_rhs_plane(aifmm_kernel* k, const double khat[3], const double e0[6], double* out);
+/* Electrostatics right-hand side: 1 V on the triangles of one conductor
+ * (ElectrostaticsMatrix::getRhs, :374-381). */
+int aifmm_kernel_rhs_conductor(aifmm_kernel* k, int conductor, double* out);
+
+/* ---- low-rank and dense components ----------------------------------------- */
+/* Partially pivoted ACA of K(rows, cols): replaces
+ * LowRank<K>::ACA_only_nodes2(row_bases, col_bases, rank, Ac, Ar)
+ * (src/ACA.cpp:639-859).  row_bases/col_bases receive up to min(nr, nc)
+ * indices into rows/cols; Ac (nr x rank) holds the original columns and Ar
+ * (rank x nc, leading dimension rank) the original rows; both buffers must
+ * hold min(nr, nc) columns/rows. */
+int aifmm_aca(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc, double tol, int* row_bases,
+              int* col_bases, int* rank, double* Ac, double* Ar);
+/* RRQR(A, TOL_POW1, TOL_POW2, partition, inputPivot, flag, fillInRank)
+ * .colPivHouseholderQRWithPartition() (src/rrqr.cpp:3-182): Q_trunc
+ * (m x rank, buffer of m x min(m, n) complex) and maxPivot.  real_mode 1
+ * selects the real Householder sign of a USE_DOUBLE build. */
+int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
+               double input_pivot, int fill_rank, int real_mode, double* Q, int* rank, double* max_pivot);
+/* X = A^{-1} B by partial-pivot LU (Eigen PartialPivLU semantics, as in
+ * EFIEMatrix::getCoefficients, src/EFIEMatrix.cpp:831-837). */
+int aifmm_lu_solve(aifmm_ctx* ctx, const double* A, int n, const double* B, int nrhs, double* X);
+
+/* ---- AIFMM solver ----------------------------------------------------------- */
+typedef struct {
+  int leaf_size;   /* inputsToSolverClass::leafSize (include/includes.hpp:73-77) */
+  int tol_pow;     /* TOL_POW: ACA tolerance 10^-tol_pow, RRQR partition-1 tolerance */
+  int fillin_tol;  /* RRQR partition-2 tolerance 10^-fillin_tol */
+  int fillin_rank; /* accepted for compatibility; the reference's active path ignores it */
+  int n_levels;    /* 0 = the reference's rule max(2, floor(log8(N / leaf))) */
+  int precision;   /* 0 = plain complex128 (the reference's arithmetic) */
+} aifmm_solver_params;
+
+typedef struct {
+  int n, n_levels, start_level, avg_leaf_size, avg_multipoles, max_rank;
+  long n_rrqr, n_compress_p2p, n_compress_p2l, n_aca, n_aca_retry, kernels;
+  double t_assemble, t_factor, t_solve; /* seconds, wall clock on the host thread */
+  double flops_factor;                  /* algorithmic flops of the factorization (complex counted) */
+  double mem_gb, mem_after_gb;          /* findMemory / findMemoryAfterFactorize */
+} aifmm_solver_info;
+
+/* AIFMM<K>::AIFMM(inputsToSolverClass, K*) (src/AIFMM.cpp:7-93): builds the
+ * octree over the kernel's unknown locations, the ACA skeletons of every box
+ * (getNodes), the L2P/P2M operators, the M2L blocks and the leaf P2P blocks,
+ * all resident in device memory. */
+int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out);
+/* AIFMM<K>::factorize() -> eliminate_phase_efficient (src/AIFMM.cpp:96-100). */
+int aifmm_solver_factorize(aifmm_solver* s);
+/* backSubstitute1/2/3 + getPhi (src/AIFMM.cpp:120-147) for nrhs right-hand
+ * sides at once: rhs and x are n x nrhs column-major complex host arrays. */
+int aifmm_solver_solve(aifmm_solver* s, const double* rhs, int nrhs, double* x);
+/* Same with device pointers (complex128, n x nrhs, ld = n). */
+int aifmm_solver_solve_device(aifmm_solver* s, const void* rhs_device, int nrhs, void* x_device);
+/* Tree statistics and phase timings (getAvgLeafSize, getAvgMultipoles,
+ * findMemory*, T:490-552 and T:4511-4571 of the tree header). */
+int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info);
+int aifmm_solver_destroy(aifmm_solver* s);
+/* Keep a device copy of the assembled, not yet factorized operator
+ * (checkpoint) and restore it (rewind) so that factorize() can run again on
+ * the same blocks, e.g. to time repeated factorizations.  No counterpart in
+ * the reference, whose tree can be factorized only once. */
+int aifmm_solver_checkpoint(aifmm_solver* s);
+int aifmm_solver_rewind(aifmm_solver* s);
+/* One record of 7 doubles per block of the tree -- level, box, kind, key,
+ * rows, cols, Frobenius norm -- for comparing two solvers' states; kinds:
+ * 0 L2P, 1 P2M, 2 M2L, 3 P2P, 4 M2P, 5 P2L, 6 L2P_f, 7 P2M_f, 8 M2M_f, 9 L2M_f.
+ * Writes at most cap records; *count receives the total. */
+int aifmm_solver_dump(aifmm_solver* s, double* out, long cap, long* count);
+
+/* Number of CUDA kernels this library has launched in the process. */
+int aifmm_launch_count(long* n);
+/* Switch per-launch CUDA-event timing of the grouped complex GEMM on (1) or
+ * off (0; also clears the record), and read the accumulated device time (ms),
+ * algorithmic flops (8 m n k per complex product) and launch count. */
+int aifmm_profile_gemm(int on);
+int aifmm_profile_gemm_read(double* ms, double* flops, long* launches);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AIFMM_B200_H */

@@ -68,6 +68,8 @@ def lib():
             "or_aifmm_solve": (_i, [_p, _dp, _dp]),
             "or_aifmm_info": (_i, [_p, _lp, _dp, _dp]),
             "or_aifmm_leaf_counts": (_i, [_p, _ip]),
+            "or_efie_set_plane_projection": (None, [_p, _i]),
+            "or_aifmm_dump": (C.c_long, [_p, _p, C.c_long]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -138,6 +140,9 @@ class EFIE(Kernel):
         h = lib().or_efie_create(nodes, mesh.n_nodes, tris, mesh.n_tris, float(freq), int(exact_lookup))
         super().__init__(h, "efie")
         self.freq = freq
+
+    def set_plane_projection(self, on: bool) -> None:
+        lib().or_efie_set_plane_projection(self.h, int(bool(on)))
 
     def rwg(self):
         t = np.zeros(6 * self.N, dtype=np.int32)
@@ -224,6 +229,13 @@ class AIFMM:
         out = np.zeros(2 * self.N, dtype=np.float64)
         _check(lib().or_aifmm_solve(self.h, _c2d(np.asarray(rhs, dtype=np.complex128)), out))
         return out.view(np.complex128).copy()
+
+    def dump(self) -> np.ndarray:
+        """(n, 7) array: level, box, kind, key, rows, cols, Frobenius norm per block."""
+        n = lib().or_aifmm_dump(self.h, None, 0)
+        out = np.zeros(7 * n, dtype=np.float64)
+        lib().or_aifmm_dump(self.h, out.ctypes.data, n)
+        return out.reshape(-1, 7)
 
     def info(self) -> dict:
         i = np.zeros(8, dtype=np.int64)

@@ -268,3 +268,34 @@ int or_aifmm_leaf_counts(void* s, int* counts) {
 }
 
 }  // extern "C"
+
+extern "C" void or_efie_set_plane_projection(void* k, int on) {
+  static_cast<EFIE*>(k)->planeProjection = (on != 0);
+}
+
+// Per-block records (level, box, kind, key, rows, cols, Frobenius norm) in the
+// same layout as aifmm_solver_dump of the GPU library.
+extern "C" long or_aifmm_dump(void* sp, double* out, long cap) {
+  Tree* t = static_cast<Solver*>(sp)->t.get();
+  long n = 0;
+  for (int j = 0; j <= t->nLevels; ++j)
+    for (int k = 0; k < (int)t->tree[j].size(); ++k) {
+      Box& B = t->tree[j][k];
+      auto add = [&](int kind, int key, const Mat& m) {
+        if (out && n < cap) {
+          double* r = out + 7 * n;
+          r[0] = j; r[1] = k; r[2] = kind; r[3] = key; r[4] = m.r; r[5] = m.c; r[6] = m.norm();
+        }
+        n++;
+      };
+      add(0, -1, B.L2P);
+      add(1, -1, B.P2M);
+      int kind = 2;
+      for (auto* mp : {&B.M2L, &B.P2P, &B.M2P, &B.P2L, &B.L2P_f, &B.P2M_f, &B.M2M_f}) {
+        for (auto& kv : *mp) add(kind, kv.first, kv.second);
+        kind++;
+      }
+      add(9, -1, B.L2M_f);
+    }
+  return n;
+}

@@ -146,6 +146,10 @@ V3 EFIE::projection(const V3& c, int s) const {
   V3 e1 = c;
   V3 n = cross(e2, e3);
   n = -1.0 * n / norm(n);
+  if (planeProjection) {
+    double d = dot(c - v1, n);
+    return c - d * n;
+  }
   double d = dot(e1, n);
   return e1 - d * n;
 }

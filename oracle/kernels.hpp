@@ -99,6 +99,10 @@ class EFIE : public Kernel {
   Phys ph;
   Mesh mesh;
   bool exactLookup = false;
+  // false (default) = the reference's projection onto the plane through the
+  // origin; true = projection onto the source triangle's own plane (used by
+  // the physics pins only, to separate that quirk from the rest).
+  bool planeProjection = false;
   int etaAnalInteg = 4;
   struct EdgeProps {
     double length;

@@ -99,9 +99,13 @@ inline void axpyC(int n, cd b, const cd* a, cd* c) {
   }
 }
 
+// Each output column is accumulated over k in increasing order by one thread,
+// so the result does not depend on the number of threads.
 inline Mat operator*(const Mat& A, const Mat& B) {
   if (A.c != B.r) fail("product dimension mismatch");
   Mat C(A.r, B.c);
+  const long work = (long)A.r * A.c * B.c;
+#pragma omp parallel for schedule(static) if (work > 200000)
   for (int j = 0; j < B.c; ++j)
     for (int k = 0; k < A.c; ++k) axpyC(A.r, B(k, j), &A.a[(size_t)k * A.r], &C.a[(size_t)j * C.r]);
   return C;
@@ -185,6 +189,8 @@ struct LU {
         const cd piv = lu(k, k);
         for (int i = k + 1; i < n; ++i) lu(i, k) /= piv;
       }
+      const long work = (long)(n - k) * (n - k);
+#pragma omp parallel for schedule(static) if (work > 100000)
       for (int j = k + 1; j < n; ++j) axpyC(n - k - 1, -lu(k, j), &lu(k + 1, k), &lu(k + 1, j));
     }
     perm.resize(n);
@@ -194,6 +200,8 @@ struct LU {
   Mat solve(const Mat& B) const {
     if (B.r != n) fail("LU solve size mismatch");
     Mat X(n, B.c);
+    const long work = (long)n * n * B.c;
+#pragma omp parallel for schedule(static) if (work > 200000)
     for (int j = 0; j < B.c; ++j) {
       cd* x = &X.a[(size_t)j * n];
       for (int i = 0; i < n; ++i) x[i] = B(perm[i], j);

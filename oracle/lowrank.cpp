@@ -185,29 +185,13 @@ static void householderVec(const Mat& R, int colj, int i, int n, bool realMode, 
   if (vn > 0) v = v * std::sqrt(2.0) / vn;
 }
 
-// One Householder step of rrqr.cpp:130-156 / 175-204 applied to R (n_rows x n_cols).
-static Mat applyReflector(const Mat& R, const Mat& h) {
-  // Rtemp = R - h * (h^H R)
-  Mat w(1, R.c);
-  for (int j = 0; j < R.c; ++j) {
-    cd s(0, 0);
-    for (int i = 0; i < R.r; ++i) s += std::conj(h(i)) * R(i, j);
-    w(0, j) = s;
-  }
-  Mat T = R;
-  for (int j = 0; j < R.c; ++j)
-    for (int i = 0; i < R.r; ++i) T(i, j) -= h(i) * w(0, j);
-  return T;
-}
-
-static void permuteCols(Mat& M, const std::vector<int>& idx) {
-  Mat T = M;
-  for (int j = 0; j < M.c; ++j)
-    for (int i = 0; i < M.r; ++i) T(i, j) = M(i, idx[j]);
-  M = T;
-}
-
-// colPivHouseholderQRWithPartition, rrqr.cpp:98-182.
+// colPivHouseholderQRWithPartition, rrqr.cpp:98-182.  The column order is
+// kept as a permutation (position -> physical column) re-sorted each step with
+// the reference's two std::sort calls, so pivot choices and ties are the
+// reference's.  A reflector is applied only to the columns at positions >= j:
+// the others are zero in rows >= j, where the reflector acts, so the values
+// are the same as applying it to all of R.  Q_trunc is formed once from the
+// committed reflectors, which equals the reference's explicit accumulation.
 void rrqrPartition(const Mat& A, int tolPow1, int tolPow2, int partition, double inputPivot, int fillInRank,
                    bool realMode, RRQRResult& out) {
   out = RRQRResult();
@@ -216,74 +200,98 @@ void rrqrPartition(const Mat& A, int tolPow1, int tolPow2, int partition, double
   const int n_rows = A.r, n_cols = A.c;
   int steps = (n_cols < n_rows) ? n_cols : n_rows;
   Mat R = A;
-  Mat Q = Mat::Identity(n_rows, n_rows);
-  Mat P = Mat::Identity(n_cols, n_cols);
+  std::vector<int> phys(n_cols);
+  std::iota(phys.begin(), phys.end(), 0);
   std::vector<double> nsq(n_cols);
   for (int j = 0; j < n_cols; ++j) {
     double s = 0.0;
     for (int i = 0; i < n_rows; ++i) s += std::norm(R(i, j));
     nsq[j] = s;
   }
+  std::vector<Mat> refl;
   double maxPivot = 0.0, mp1 = 0.0, mp2 = 0.0;
   int rank_partition1 = std::min(partition, n_rows);
-  auto step = [&](int j, int endSort) {
+  auto sortStep = [&](int j, int endSort) {
     std::vector<int> idx(nsq.size());
     std::iota(idx.begin(), idx.end(), 0);
     std::sort(idx.begin() + j, idx.begin() + endSort, [&](int i1, int i2) { return nsq[i1] > nsq[i2]; });
     std::sort(nsq.begin() + j, nsq.begin() + endSort, std::greater<double>());
-    permuteCols(R, idx);
-    permuteCols(P, idx);
+    std::vector<int> np = phys;
+    for (int q = j; q < endSort; ++q) np[q] = phys[idx[q]];
+    phys = np;
+  };
+  // Householder vector of the column at position j and w_q = h^H R(:, phys[q])
+  // for q >= j; returns the would-be pivot R(j, phys[j]) after the reflection.
+  std::vector<cd> w(n_cols);
+  auto reflect = [&](int j, Mat& h) -> cd {
+    householderVec(R, phys[j], j, n_rows, realMode, h);
+    for (int q = j; q < n_cols; ++q) {
+      const int c = phys[q];
+      cd s(0, 0);
+      for (int i = j; i < n_rows; ++i) s += std::conj(h(i)) * R(i, c);
+      w[q] = s;
+    }
+    return R(j, phys[j]) - h(j) * w[j];
+  };
+  auto commit = [&](int j, const Mat& h) {
+    for (int q = j; q < n_cols; ++q) {
+      const int c = phys[q];
+      for (int i = j; i < n_rows; ++i) R(i, c) -= h(i) * w[q];
+    }
+    for (int i = j + 1; i < n_rows; ++i) R(i, phys[j]) = 0.0;
+    refl.push_back(h);
+    for (int q = j + 1; q < n_cols; ++q) nsq[q] = nsq[q] - std::abs(R(j, phys[q])) * std::abs(R(j, phys[q]));
   };
   for (int j = 0; j < rank_partition1; ++j) {
-    step(j, partition);
+    sortStep(j, partition);
     Mat h;
-    householderVec(R, j, j, n_rows, realMode, h);
-    Mat Rt = applyReflector(R, h);
-    if (j == 0) mp1 = std::abs(Rt(j, j));
+    const cd rjj = reflect(j, h);
+    if (j == 0) mp1 = std::abs(rjj);
     maxPivot = mp1;
-    double pivot = std::abs(Rt(j, j));
+    const double pivot = std::abs(rjj);
     if (pivot / mp1 < tolerance1) {
       rank_partition1 = j - 1;  // reference quirk (rrqr.cpp:116)
       break;
     }
-    R = Rt;
-    for (int i = j + 1; i < n_rows; ++i) R(i, j) = 0.0;
-    // Q = Q - (Q h) h^H
-    Mat Qh = Q * h;
-    for (int c = 0; c < n_rows; ++c)
-      for (int r = 0; r < n_rows; ++r) Q(r, c) -= Qh(r) * std::conj(h(c));
-    for (int i = j + 1; i < n_cols; ++i) nsq[i] = nsq[i] - std::abs(R(j, i)) * std::abs(R(j, i));
+    commit(j, h);
   }
   for (int i = rank_partition1; i < partition; ++i) nsq[i] = 0.0;
   steps = steps - (partition - rank_partition1);
   const int first = rank_partition1;
   int rank_partition2 = std::min(steps - first, n_rows);
   for (int j = first; j < steps; ++j) {
-    step(j, n_cols);
+    sortStep(j, n_cols);
     Mat h;
-    householderVec(R, j, j, n_rows, realMode, h);
-    Mat Rt = applyReflector(R, h);
+    const cd rjj = reflect(j, h);
     if (j == first) {
-      mp2 = std::abs(Rt(first, first));
+      mp2 = std::abs(rjj);
       maxPivot = std::max(inputPivot, mp2);
     }
-    double pivot = std::abs(Rt(j, j));
+    const double pivot = std::abs(rjj);
     if (pivot / maxPivot < tolerance2 || j - first >= fillInRank) {
       rank_partition2 = j - first;
       break;
     }
-    R = Rt;
-    for (int i = j + 1; i < n_rows; ++i) R(i, j) = 0.0;
-    Mat Qh = Q * h;
-    for (int c = 0; c < n_rows; ++c)
-      for (int r = 0; r < n_rows; ++r) Q(r, c) -= Qh(r) * std::conj(h(c));
-    for (int i = j + 1; i < n_cols; ++i) nsq[i] = nsq[i] - std::abs(R(j, i)) * std::abs(R(j, i));
+    commit(j, h);
   }
   const int rank_A = rank_partition1 + rank_partition2;
   if (rank_A < 0 || rank_A > n_rows) fail("RRQR rank out of range");
-  out.Q = Q.block(0, 0, n_rows, rank_A);
-  out.R = R.block(0, 0, rank_A, n_cols);
-  out.P = P;
+  // Q_trunc = H_0 H_1 ... H_{t-1} [I; 0]
+  Mat Q = Mat::Identity(n_rows, rank_A);
+  for (int r = (int)refl.size() - 1; r >= 0; --r) {
+    const Mat& h = refl[r];
+    for (int c = 0; c < rank_A; ++c) {
+      cd s(0, 0);
+      for (int i = 0; i < n_rows; ++i) s += std::conj(h(i)) * Q(i, c);
+      for (int i = 0; i < n_rows; ++i) Q(i, c) -= h(i) * s;
+    }
+  }
+  out.Q = Q;
+  out.R = Mat(rank_A, n_cols);
+  for (int q = 0; q < n_cols; ++q)
+    for (int i = 0; i < rank_A; ++i) out.R(i, q) = R(i, phys[q]);
+  out.P = Mat(n_cols, n_cols);
+  for (int q = 0; q < n_cols; ++q) out.P(phys[q], q) = 1.0;
   out.rank = rank_A;
   out.maxPivot = maxPivot;
   out.maxPivotPartition1 = mp1;

@@ -1,0 +1,315 @@
+// C ABI of libaifmm_b200.so: argument checking, error translation and the
+// context / kernel objects.  Numerical work happens in the kernels of
+// assemble.cu and the solver files; nothing here computes on the host.
+#include <atomic>
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "context.cuh"
+
+namespace aifmm {
+
+static thread_local std::string g_last_error;
+void set_last_error(const std::string& msg) { g_last_error = msg; }
+static std::atomic<long> g_launches{0};
+void count_launch(long n) { g_launches += n; }
+long launch_count() { return g_launches.load(); }
+
+static std::mutex g_ctx_mu;
+
+void ctx_retain(aifmm_ctx* c) {
+  std::lock_guard<std::mutex> l(g_ctx_mu);
+  c->refs++;
+}
+
+void ctx_release(aifmm_ctx* c) {
+  bool last;
+  {
+    std::lock_guard<std::mutex> l(g_ctx_mu);
+    last = (--c->refs == 0);
+  }
+  if (!last) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->pool) cudaMemPoolDestroy(c->pool);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c;
+}
+
+void DevBuf::alloc(aifmm_ctx* c, size_t n) {
+  release();
+  ctx = c;
+  bytes = n;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    cudaGetLastError();
+    throw Error(AIFMM_ENOMEM, "device allocation of " + std::to_string(n) + " bytes failed: " + cudaGetErrorString(e));
+  }
+  c->bytes_live += n;
+}
+void DevBuf::release() {
+  if (p && ctx) {
+    cudaFreeAsync(p, ctx->stream);
+    ctx->bytes_live -= bytes;
+  }
+  p = nullptr;
+  bytes = 0;
+}
+
+}  // namespace aifmm
+
+using namespace aifmm;
+
+#define API_BEGIN try {
+#define API_END                                  \
+  }                                              \
+  catch (const Error& e) {                       \
+    set_last_error(e.what());                    \
+    return e.code;                               \
+  }                                              \
+  catch (const std::bad_alloc&) {                \
+    set_last_error("host allocation failed");    \
+    return AIFMM_ENOMEM;                         \
+  }                                              \
+  catch (const std::exception& e) {              \
+    set_last_error(e.what());                    \
+    return AIFMM_EINVAL;                         \
+  }                                              \
+  return AIFMM_OK;
+
+extern "C" {
+
+const char* aifmm_last_error(void) { return g_last_error.c_str(); }
+
+int aifmm_launch_count(long* n) {
+  if (!n) return AIFMM_EINVAL;
+  *n = launch_count();
+  return AIFMM_OK;
+}
+
+int aifmm_ctx_create(int device, aifmm_ctx** out) {
+  API_BEGIN
+  AIFMM_REQUIRE(out, AIFMM_EINVAL, "out is NULL");
+  int n = 0;
+  AIFMM_CUDA(cudaGetDeviceCount(&n));
+  AIFMM_REQUIRE(device >= 0 && device < n, AIFMM_EINVAL, "no such CUDA device");
+  AIFMM_CUDA(cudaSetDevice(device));
+  std::unique_ptr<aifmm_ctx> c(new aifmm_ctx);
+  c->device = device;
+  AIFMM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+  cudaMemPoolProps props{};
+  props.allocType = cudaMemAllocationTypePinned;
+  props.location.type = cudaMemLocationTypeDevice;
+  props.location.id = device;
+  AIFMM_CUDA(cudaMemPoolCreate(&c->pool, &props));
+  uint64_t thresh = UINT64_MAX;  // keep freed blocks for reuse
+  AIFMM_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+  *out = c.release();
+  API_END
+}
+
+int aifmm_ctx_destroy(aifmm_ctx* ctx) {
+  API_BEGIN
+  if (!ctx) return AIFMM_OK;
+  AIFMM_REQUIRE(!ctx->closed, AIFMM_ESTATE, "context destroyed twice");
+  ctx->closed = true;
+  ctx_release(ctx);
+  API_END
+}
+
+int aifmm_ctx_synchronize(aifmm_ctx* ctx) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx, AIFMM_EINVAL, "ctx is NULL");
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int aifmm_ctx_stream(aifmm_ctx* ctx, void** stream) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx && stream, AIFMM_EINVAL, "NULL argument");
+  *stream = (void*)ctx->stream;
+  API_END
+}
+
+int aifmm_kernel_create_efie(aifmm_ctx* ctx, const double* nodes, int n_nodes, const int* tris, int n_tris,
+                             double freq, aifmm_kernel** out) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx && nodes && tris && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(n_nodes > 0 && n_tris > 0, AIFMM_EINVAL, "empty mesh");
+  AIFMM_REQUIRE(freq > 0 && std::isfinite(freq), AIFMM_EINVAL, "frequency must be positive");
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  EfieHostTables h;
+  build_efie_tables(nodes, n_nodes, tris, n_tris, h);
+  AIFMM_REQUIRE(!h.len.empty(), AIFMM_EINVAL, "mesh has no RWG (shared) edges");
+  std::unique_ptr<aifmm_kernel> k(new aifmm_kernel);
+  k->ctx = ctx;
+  k->d_tri = upload(ctx, h.tri);
+  k->d_node = upload(ctx, h.node);
+  k->d_rwg = upload(ctx, h.rwg);
+  k->d_len = upload(ctx, h.len);
+  k->d_side = upload(ctx, h.side);
+  k->locations = h.locations;
+  k->rwg_host = h.rwg;
+  k->edge_host = h.edge;
+  KernelGeom& g = k->geom;
+  g.efie = true;
+  g.N = (int)h.len.size();
+  EfieGeom& e = g.ge;
+  e.N = g.N;
+  e.nt = n_tris;
+  e.tri = k->d_tri.as<double>();
+  e.node = k->d_node.as<double>();
+  e.rwg = k->d_rwg.as<int4>();
+  e.len = k->d_len.as<double>();
+  e.side = k->d_side.as<double>();
+  // include/includes.hpp:53-63 with a runtime frequency
+  const double PI = 4.0 * std::atan(1.0);
+  const double c = 3.0e8, lambda = c / freq;
+  e.PI = PI;
+  e.freq = freq;
+  e.eps = 8.854187817e-12;
+  e.mu = 4 * PI * 1e-7;
+  e.kappa = 2 * PI / lambda;
+  e.c4 = -1.0 / 4.0 / PI;
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx_retain(ctx);
+  *out = k.release();
+  API_END
+}
+
+int aifmm_kernel_create_es(aifmm_ctx* ctx, const double* nodes, int n_nodes, const int* tris, const int* cond,
+                           int n_tris, aifmm_kernel** out) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx && nodes && tris && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(n_nodes > 0 && n_tris > 0, AIFMM_EINVAL, "empty mesh");
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  std::vector<double> tri, loc;
+  build_es_tables(nodes, n_nodes, tris, n_tris, tri, loc);
+  std::unique_ptr<aifmm_kernel> k(new aifmm_kernel);
+  k->ctx = ctx;
+  k->d_tri = upload(ctx, tri);
+  k->locations = loc;
+  k->cond.assign(n_tris, 1);
+  if (cond) k->cond.assign(cond, cond + n_tris);
+  KernelGeom& g = k->geom;
+  g.efie = false;
+  g.N = n_tris;
+  g.gs.N = n_tris;
+  g.gs.tri = k->d_tri.as<double>();
+  const double PI = 4.0 * std::atan(1.0);
+  g.gs.C0 = 1.0 / (4 * PI * 8.854187817e-12);
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  ctx_retain(ctx);
+  *out = k.release();
+  API_END
+}
+
+int aifmm_kernel_destroy(aifmm_kernel* k) {
+  API_BEGIN
+  if (!k) return AIFMM_OK;
+  aifmm_ctx* c = k->ctx;
+  cudaSetDevice(c->device);
+  delete k;  // frees the kernel's device tables on the context stream
+  ctx_release(c);
+  API_END
+}
+
+int aifmm_kernel_set_plane_projection(aifmm_kernel* k, int on) {
+  API_BEGIN
+  AIFMM_REQUIRE(k, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(k->geom.efie, AIFMM_EINVAL, "not an EFIE kernel");
+  k->geom.ge.plane_projection = on ? 1 : 0;
+  API_END
+}
+
+int aifmm_kernel_size(const aifmm_kernel* k, int* n) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && n, AIFMM_EINVAL, "NULL argument");
+  *n = k->geom.N;
+  API_END
+}
+
+int aifmm_kernel_locations(const aifmm_kernel* k, double* xyz) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && xyz, AIFMM_EINVAL, "NULL argument");
+  std::memcpy(xyz, k->locations.data(), k->locations.size() * sizeof(double));
+  API_END
+}
+
+static void check_ids(const int* ids, int n, int N, const char* what) {
+  for (int i = 0; i < n; ++i)
+    AIFMM_REQUIRE(ids[i] >= 0 && ids[i] < N, AIFMM_EINVAL, std::string(what) + " index out of range");
+}
+
+int aifmm_kernel_matrix(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc, int precision, void* out,
+                        int ld) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && rows && cols && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(nr >= 0 && nc >= 0 && ld >= nr, AIFMM_EINVAL, "bad sizes");
+  AIFMM_REQUIRE(precision == 0 || precision == 1, AIFMM_EINVAL, "precision must be 0 or 1");
+  if (nr == 0 || nc == 0) return AIFMM_OK;
+  check_ids(rows, nr, k->geom.N, "row");
+  check_ids(cols, nc, k->geom.N, "column");
+  aifmm_ctx* c = k->ctx;
+  AIFMM_CUDA(cudaSetDevice(c->device));
+  const size_t esz = precision == 0 ? sizeof(zd) : sizeof(zf);
+  DevBuf dr(c, sizeof(int) * nr), dc(c, sizeof(int) * nc), dout(c, esz * (size_t)ld * nc);
+  AIFMM_CUDA(cudaMemcpyAsync(dr.p, rows, sizeof(int) * nr, cudaMemcpyHostToDevice, c->stream));
+  AIFMM_CUDA(cudaMemcpyAsync(dc.p, cols, sizeof(int) * nc, cudaMemcpyHostToDevice, c->stream));
+  launch_gather(k->geom, dr.as<int>(), nr, dc.as<int>(), nc, precision, dout.p, ld, c->stream);
+  AIFMM_CUDA(cudaMemcpyAsync(out, dout.p, esz * (size_t)ld * nc, cudaMemcpyDeviceToHost, c->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(c->stream));
+  API_END
+}
+
+int aifmm_kernel_matrix_device(aifmm_kernel* k, const int* rows_device, int nr, const int* cols_device, int nc,
+                               int precision, void* out_device, int ld) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && rows_device && cols_device && out_device, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(nr >= 0 && nc >= 0 && ld >= nr, AIFMM_EINVAL, "bad sizes");
+  AIFMM_REQUIRE(precision == 0 || precision == 1, AIFMM_EINVAL, "precision must be 0 or 1");
+  AIFMM_CUDA(cudaSetDevice(k->ctx->device));
+  launch_gather(k->geom, rows_device, nr, cols_device, nc, precision, out_device, ld, k->ctx->stream);
+  API_END
+}
+
+int aifmm_kernel_rhs_reference(aifmm_kernel* k, const double einc[3], double* out) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && einc && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(k->geom.efie, AIFMM_EINVAL, "not an EFIE kernel");
+  aifmm_ctx* c = k->ctx;
+  AIFMM_CUDA(cudaSetDevice(c->device));
+  DevBuf d(c, sizeof(zd) * k->geom.N);
+  launch_rhs_reference(k->geom, einc, d.as<zd>(), c->stream);
+  AIFMM_CUDA(cudaMemcpyAsync(out, d.p, sizeof(zd) * k->geom.N, cudaMemcpyDeviceToHost, c->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(c->stream));
+  API_END
+}
+
+int aifmm_kernel_rhs_plane(aifmm_kernel* k, const double khat[3], const double e0[6], double* out) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && khat && e0 && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(k->geom.efie, AIFMM_EINVAL, "not an EFIE kernel");
+  aifmm_ctx* c = k->ctx;
+  AIFMM_CUDA(cudaSetDevice(c->device));
+  DevBuf d(c, sizeof(zd) * k->geom.N);
+  launch_rhs_plane(k->geom, khat, e0, d.as<zd>(), c->stream);
+  AIFMM_CUDA(cudaMemcpyAsync(out, d.p, sizeof(zd) * k->geom.N, cudaMemcpyDeviceToHost, c->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(c->stream));
+  API_END
+}
+
+int aifmm_kernel_rhs_conductor(aifmm_kernel* k, int conductor, double* out) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(!k->geom.efie, AIFMM_EINVAL, "not an electrostatics kernel");
+  for (int i = 0; i < k->geom.N; ++i) {  // a 0/1 indicator vector: no arithmetic to offload
+    out[2 * i] = (k->cond[i] == conductor) ? 1.0 : 0.0;
+    out[2 * i + 1] = 0.0;
+  }
+  API_END
+}
+
+}  // extern "C"

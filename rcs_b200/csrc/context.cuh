@@ -1,0 +1,72 @@
+// Library context: one device, one stream, a stream-ordered device memory
+// pool, and the kernel (mesh) objects.
+#pragma once
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "assemble.cuh"
+
+// Objects created on a context (kernels, solvers) hold a reference; the
+// context's stream and memory pool are released when aifmm_ctx_destroy has
+// been called and the last such object is gone, so destruction order does
+// not matter to callers.
+struct aifmm_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  cudaMemPool_t pool = nullptr;
+  size_t bytes_live = 0;
+  int refs = 1;          // the creator's reference
+  bool closed = false;
+};
+
+namespace aifmm {
+void ctx_retain(aifmm_ctx* c);
+void ctx_release(aifmm_ctx* c);
+}  // namespace aifmm
+
+namespace aifmm {
+
+// Device buffer allocated from the context's stream-ordered pool.
+struct DevBuf {
+  aifmm_ctx* ctx = nullptr;
+  void* p = nullptr;
+  size_t bytes = 0;
+  DevBuf() {}
+  DevBuf(aifmm_ctx* c, size_t n) { alloc(c, n); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf& operator=(DevBuf&& o) noexcept {
+    if (this != &o) {
+      release();
+      ctx = o.ctx; p = o.p; bytes = o.bytes;
+      o.p = nullptr; o.bytes = 0;
+    }
+    return *this;
+  }
+  ~DevBuf() { release(); }
+  void alloc(aifmm_ctx* c, size_t n);
+  void release();
+  template <typename T>
+  T* as() const { return static_cast<T*>(p); }
+};
+
+template <typename T>
+DevBuf upload(aifmm_ctx* c, const std::vector<T>& v) {
+  DevBuf b(c, std::max<size_t>(1, v.size() * sizeof(T)));
+  if (!v.empty()) AIFMM_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  return b;
+}
+
+}  // namespace aifmm
+
+struct aifmm_kernel {
+  aifmm_ctx* ctx = nullptr;
+  aifmm::KernelGeom geom;
+  aifmm::DevBuf d_tri, d_node, d_rwg, d_len, d_side;
+  std::vector<double> locations;   // N x 3
+  std::vector<int> cond;           // electrostatics: conductor per triangle
+  std::vector<int> rwg_host;       // EFIE: N x 4
+  std::vector<int> edge_host;      // EFIE: N x 2
+};

@@ -1,0 +1,423 @@
+// Dense complex128 kernels: grouped SIMT GEMM (64x64 tiles, 4x4 complex
+// micro-tiles per thread), blocked LU with a single-CTA panel, blocked
+// triangular solves, batched copies and norms.
+#include <algorithm>
+
+#include "dense.cuh"
+
+namespace aifmm {
+
+// ------------------------------------------------------------------ GEMM
+constexpr int GBM = 64, GBN = 64, GBK = 8;
+
+struct GemmTile {
+  int prob, tm, tn, pad;
+};
+
+__device__ __forceinline__ zd ldA(const GemmProblem& P, int i, int k) {
+  if (i >= P.m || k >= P.k) return zmk(0, 0);
+  if (P.opA == OP_N) return P.A[(size_t)k * P.lda + i];
+  return zconj(P.A[(size_t)i * P.lda + k]);
+}
+__device__ __forceinline__ zd ldB(const GemmProblem& P, int k, int j) {
+  if (k >= P.k || j >= P.n) return zmk(0, 0);
+  if (P.opB == OP_N) return P.B[(size_t)j * P.ldb + k];
+  return zconj(P.B[(size_t)k * P.ldb + j]);
+}
+
+__global__ void __launch_bounds__(256) zgemm_grouped_kernel(const GemmProblem* __restrict__ probs,
+                                                            const GemmTile* __restrict__ tiles) {
+  __shared__ zd As[2][GBK][GBM];
+  __shared__ zd Bs[2][GBK][GBN];
+  const GemmTile T = tiles[blockIdx.x];
+  const GemmProblem P = probs[T.prob];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int row0 = T.tm * GBM, col0 = T.tn * GBN;
+  // load mapping: A tile 64x8 -> thread loads (i = t%64, k = t/64) and (i, k+4)
+  //               B tile 8x64 -> thread loads (k = t%8, j = t/8) and (k, j+32)
+  const int t = threadIdx.x;
+  const int ai = t & 63, ak = t >> 6;
+  const int bk = t & 7, bj = t >> 3;
+  zd acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = zmk(0, 0);
+  zd ra0 = ldA(P, row0 + ai, ak), ra1 = ldA(P, row0 + ai, ak + 4);
+  zd rb0 = ldB(P, bk, col0 + bj), rb1 = ldB(P, bk, col0 + bj + 32);
+  int buf = 0;
+  for (int k0 = 0; k0 < P.k; k0 += GBK) {
+    As[buf][ak][ai] = ra0;
+    As[buf][ak + 4][ai] = ra1;
+    Bs[buf][bk][bj] = rb0;
+    Bs[buf][bk][bj + 32] = rb1;
+    __syncthreads();
+    const int kn = k0 + GBK;
+    if (kn < P.k) {  // prefetch the next K slice while computing this one
+      ra0 = ldA(P, row0 + ai, kn + ak);
+      ra1 = ldA(P, row0 + ai, kn + ak + 4);
+      rb0 = ldB(P, kn + bk, col0 + bj);
+      rb1 = ldB(P, kn + bk, col0 + bj + 32);
+    }
+#pragma unroll
+    for (int kk = 0; kk < GBK; ++kk) {
+      zd a[4], b[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          acc[i][j].x = fma(a[i].x, b[j].x, acc[i][j].x);
+          acc[i][j].x = fma(-a[i].y, b[j].y, acc[i][j].x);
+          acc[i][j].y = fma(a[i].x, b[j].y, acc[i][j].y);
+          acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
+        }
+    }
+    buf ^= 1;
+  }
+  const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
+#pragma unroll
+  for (int i = 0; i < 4; ++i) {
+    const int r = row0 + tx + 16 * i;
+    if (r >= P.m) continue;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      const int c = col0 + ty + 16 * j;
+      if (c >= P.n) continue;
+      zd* cp = P.C + (size_t)c * P.ldc + r;
+      zd v = zmul(P.alpha, acc[i][j]);
+      if (!beta0) v = zadd(v, zmul(P.beta, *cp));
+      *cp = v;
+    }
+  }
+}
+
+// Optional per-launch timing of the grouped GEMM (events on the launching
+// stream) for the roofline figure; off unless a caller enables it.
+struct GemmProfile {
+  bool on = false;
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  double flops = 0;
+  long launches = 0;
+};
+static GemmProfile g_prof;
+
+void gemm_profile_enable(bool on) {
+  for (auto& e : g_prof.ev) {
+    cudaEventDestroy(e.first);
+    cudaEventDestroy(e.second);
+  }
+  g_prof = GemmProfile();
+  g_prof.on = on;
+}
+
+void gemm_profile_read(double* ms, double* flops, long* launches) {
+  double t = 0;
+  for (auto& e : g_prof.ev) {
+    AIFMM_CUDA(cudaEventSynchronize(e.second));
+    float x = 0;
+    AIFMM_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+    t += x;
+  }
+  *ms = t;
+  *flops = g_prof.flops;
+  *launches = g_prof.launches;
+}
+
+void zgemm_grouped(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs) {
+  std::vector<GemmProblem> ps;
+  std::vector<GemmTile> tiles;
+  ps.reserve(probs.size());
+  for (const GemmProblem& p : probs) {
+    if (p.m <= 0 || p.n <= 0) continue;
+    if (p.k <= 0) {  // C = beta C
+      if (!(p.beta.x == 1.0 && p.beta.y == 0.0)) {
+        CopyProblem c{p.C, p.C, p.m, p.n, p.ldc, p.ldc, 0, p.beta};
+        zcopy_grouped(ctx, {c});
+      }
+      continue;
+    }
+    const int pi = (int)ps.size();
+    ps.push_back(p);
+    const int tm = (p.m + GBM - 1) / GBM, tn = (p.n + GBN - 1) / GBN;
+    for (int a = 0; a < tm; ++a)
+      for (int b = 0; b < tn; ++b) tiles.push_back({pi, a, b, 0});
+  }
+  if (tiles.empty()) return;
+  AIFMM_REQUIRE(tiles.size() < (size_t)INT32_MAX, AIFMM_EOVERFLOW, "too many GEMM tiles");
+  DevBuf dp = upload(ctx, ps), dt = upload(ctx, tiles);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (g_prof.on) {
+    AIFMM_CUDA(cudaEventCreate(&e0));
+    AIFMM_CUDA(cudaEventCreate(&e1));
+    AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
+  }
+  zgemm_grouped_kernel<<<(unsigned)tiles.size(), 256, 0, ctx->stream>>>(dp.as<GemmProblem>(), dt.as<GemmTile>());
+  AIFMM_LAUNCHED();
+  if (g_prof.on) {
+    AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
+    g_prof.ev.push_back({e0, e1});
+    for (const GemmProblem& p : ps) g_prof.flops += 8.0 * p.m * (double)p.n * p.k;
+    g_prof.launches++;
+  }
+}
+
+// ------------------------------------------------------------------ copies
+__global__ void zcopy_grouped_kernel(const CopyProblem* __restrict__ probs, int nprob, const long* __restrict__ start,
+                                     long total) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+      int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const CopyProblem& P = probs[lo];
+    const long u = t - start[lo];
+    const int i = (int)(u % P.rows), j = (int)(u / P.rows);
+    zd v = P.conjTrans ? zconj(P.src[(size_t)i * P.lds + j]) : P.src[(size_t)j * P.lds + i];
+    P.dst[(size_t)j * P.ldd + i] = zmul(P.scale, v);
+  }
+}
+
+void zcopy_grouped(aifmm_ctx* ctx, const std::vector<CopyProblem>& probs) {
+  std::vector<CopyProblem> ps;
+  std::vector<long> start;
+  long total = 0;
+  for (const CopyProblem& p : probs) {
+    if (p.rows <= 0 || p.cols <= 0) continue;
+    ps.push_back(p);
+    start.push_back(total);
+    total += (long)p.rows * p.cols;
+  }
+  if (ps.empty()) return;
+  DevBuf dp = upload(ctx, ps), ds = upload(ctx, start);
+  const int grid = (int)std::min<long>((total + 255) / 256, 148L * 32);
+  zcopy_grouped_kernel<<<grid, 256, 0, ctx->stream>>>(dp.as<CopyProblem>(), (int)ps.size(), ds.as<long>(), total);
+  AIFMM_LAUNCHED();
+}
+
+__global__ void zfill_kernel(zd* p, size_t n, zd v) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) p[i] = v;
+}
+void zfill(aifmm_ctx* ctx, zd* p, size_t n, zd v) {
+  if (n == 0) return;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 32);
+  zfill_kernel<<<grid, 256, 0, ctx->stream>>>(p, n, v);
+  AIFMM_LAUNCHED();
+}
+
+__global__ void zident_kernel(zd* p, int rows, int cols, zd diag) {
+  const size_t n = (size_t)rows * cols;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n; t += (size_t)gridDim.x * blockDim.x) {
+    const int i = (int)(t % rows), j = (int)(t / rows);
+    p[t] = (i == j) ? diag : zmk(0, 0);
+  }
+}
+void zset_identity(aifmm_ctx* ctx, zd* p, int rows, int cols, zd diag) {
+  const size_t n = (size_t)rows * cols;
+  if (n == 0) return;
+  const int grid = (int)std::min<size_t>((n + 255) / 256, 148 * 32);
+  zident_kernel<<<grid, 256, 0, ctx->stream>>>(p, rows, cols, diag);
+  AIFMM_LAUNCHED();
+}
+
+// ------------------------------------------------------------------ norms
+__global__ void znorm_kernel(const NormProblem* __restrict__ probs, double* out) {
+  const NormProblem P = probs[blockIdx.x];
+  double s = 0.0;
+  const size_t n = (size_t)P.rows * P.cols;
+  for (size_t t = threadIdx.x; t < n; t += blockDim.x) {
+    const int i = (int)(t % P.rows), j = (int)(t / P.rows);
+    s += zabs2(P.p[(size_t)j * P.ld + i]);
+  }
+  __shared__ double red[32];
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffff, s, o);
+  if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    s = (threadIdx.x < blockDim.x / 32) ? red[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffff, s, o);
+    if (threadIdx.x == 0) out[blockIdx.x] = sqrt(s);
+  }
+}
+void znorm_grouped(aifmm_ctx* ctx, const std::vector<NormProblem>& probs, double* out_dev) {
+  if (probs.empty()) return;
+  DevBuf dp = upload(ctx, probs);
+  znorm_kernel<<<(unsigned)probs.size(), 256, 0, ctx->stream>>>(dp.as<NormProblem>(), out_dev);
+  AIFMM_LAUNCHED();
+}
+
+// ------------------------------------------------------------------ LU
+constexpr int LU_NB = 32;
+
+// Factor columns [j0, j0+nb) of the n x n matrix: pivot search over the whole
+// column below the diagonal (largest |a|, lowest row on ties), full-row
+// swaps, division by the pivot, rank-1 update inside the panel.
+__global__ void __launch_bounds__(1024) zgetrf_panel_kernel(zd* A, int n, int lda, int j0, int nb, int* piv,
+                                                             int* info) {
+  __shared__ double sv[32];
+  __shared__ int si[32];
+  __shared__ int s_p;
+  __shared__ zd s_piv;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  for (int k = j0; k < j0 + nb; ++k) {
+    // pivot search
+    double best = -1.0;
+    int bi = n;
+    for (int i = k + tid; i < n; i += nt) {
+      const double v = hypot(A[(size_t)k * lda + i].x, A[(size_t)k * lda + i].y);
+      if (v > best) { best = v; bi = i; }
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ov = __shfl_xor_sync(0xffffffff, best, o);
+      const int oi = __shfl_xor_sync(0xffffffff, bi, o);
+      if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+    }
+    if ((tid & 31) == 0) { sv[tid >> 5] = best; si[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid < 32) {
+      best = (tid < (nt >> 5)) ? sv[tid] : -1.0;
+      bi = (tid < (nt >> 5)) ? si[tid] : n;
+      for (int o = 16; o > 0; o >>= 1) {
+        const double ov = __shfl_xor_sync(0xffffffff, best, o);
+        const int oi = __shfl_xor_sync(0xffffffff, bi, o);
+        if (ov > best || (ov == best && oi < bi)) { best = ov; bi = oi; }
+      }
+      if (tid == 0) {
+        s_p = (best > 0.0) ? bi : -1;
+        piv[k] = (best > 0.0) ? bi : k;
+        if (best <= 0.0 && *info == 0) *info = k + 1;
+      }
+    }
+    __syncthreads();
+    const int p = s_p;
+    if (p >= 0 && p != k)
+      for (int j = tid; j < n; j += nt) {
+        zd a = A[(size_t)j * lda + k];
+        A[(size_t)j * lda + k] = A[(size_t)j * lda + p];
+        A[(size_t)j * lda + p] = a;
+      }
+    __syncthreads();
+    if (tid == 0) s_piv = A[(size_t)k * lda + k];
+    __syncthreads();
+    if (p >= 0)
+      for (int i = k + 1 + tid; i < n; i += nt) A[(size_t)k * lda + i] = zdiv(A[(size_t)k * lda + i], s_piv);
+    __syncthreads();
+    // rank-1 update of the remaining panel columns
+    const int ncol = j0 + nb - k - 1, nrow = n - k - 1;
+    for (int t = tid; t < ncol * nrow; t += nt) {
+      const int i = k + 1 + t % nrow, j = k + 1 + t / nrow;
+      A[(size_t)j * lda + i] = zsub(A[(size_t)j * lda + i], zmul(A[(size_t)k * lda + i], A[(size_t)j * lda + k]));
+    }
+    __syncthreads();
+  }
+}
+
+// X <- T^{-1} X for a triangular nb x nb block T (unit lower or non-unit
+// upper) and X = nb rows x ncols columns; one thread per column.
+template <bool LOWER_UNIT>
+__global__ void ztrsm_block_kernel(const zd* __restrict__ T, int ldt, int nb, zd* X, int ldx, int ncols) {
+  __shared__ zd Ts[LU_NB * LU_NB];
+  for (int t = threadIdx.x; t < nb * nb; t += blockDim.x) Ts[t] = T[(size_t)(t / nb) * ldt + (t % nb)];
+  __syncthreads();
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncols) return;
+  zd x[LU_NB];
+#pragma unroll
+  for (int i = 0; i < LU_NB; ++i)
+    if (i < nb) x[i] = X[(size_t)c * ldx + i];
+  if (LOWER_UNIT) {
+#pragma unroll
+    for (int i = 0; i < LU_NB; ++i) {
+      if (i >= nb) break;
+#pragma unroll
+      for (int l = 0; l < LU_NB; ++l)
+        if (l < i) x[i] = zsub(x[i], zmul(Ts[l * nb + i], x[l]));
+    }
+  } else {
+#pragma unroll
+    for (int i = LU_NB - 1; i >= 0; --i) {
+      if (i >= nb) continue;
+#pragma unroll
+      for (int l = 0; l < LU_NB; ++l)
+        if (l > i && l < nb) x[i] = zsub(x[i], zmul(Ts[l * nb + i], x[l]));
+      x[i] = zdiv(x[i], Ts[i * nb + i]);
+    }
+  }
+#pragma unroll
+  for (int i = 0; i < LU_NB; ++i)
+    if (i < nb) X[(size_t)c * ldx + i] = x[i];
+}
+
+__global__ void zlaswp_kernel(zd* B, int ldb, int nrhs, const int* __restrict__ piv, int n) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= nrhs) return;
+  zd* b = B + (size_t)c * ldb;
+  for (int k = 0; k < n; ++k) {
+    const int p = piv[k];
+    if (p != k) {
+      zd t = b[k];
+      b[k] = b[p];
+      b[p] = t;
+    }
+  }
+}
+
+void zgetrf(aifmm_ctx* ctx, zd* A, int n, int lda, int* piv, int* info) {
+  if (n <= 0) return;
+  AIFMM_CUDA(cudaMemsetAsync(info, 0, sizeof(int), ctx->stream));
+  for (int j0 = 0; j0 < n; j0 += LU_NB) {
+    const int nb = std::min(LU_NB, n - j0);
+    zgetrf_panel_kernel<<<1, 1024, 0, ctx->stream>>>(A, n, lda, j0, nb, piv, info);
+    AIFMM_LAUNCHED();
+    const int rest = n - j0 - nb;
+    if (rest <= 0) continue;
+    // U12 = L11^{-1} A12
+    ztrsm_block_kernel<true><<<ceil_div(rest, 128), 128, 0, ctx->stream>>>(A + (size_t)j0 * lda + j0, lda, nb,
+                                                                           A + (size_t)(j0 + nb) * lda + j0, lda,
+                                                                           rest);
+    AIFMM_LAUNCHED();
+    // A22 -= L21 U12
+    GemmProblem g{A + (size_t)j0 * lda + j0 + nb, A + (size_t)(j0 + nb) * lda + j0, A + (size_t)(j0 + nb) * lda + j0 + nb,
+                  rest, rest, nb, lda, lda, lda, OP_N, OP_N, zmk(-1, 0), zmk(1, 0)};
+    zgemm_grouped(ctx, {g});
+  }
+}
+
+void zgetrs(aifmm_ctx* ctx, const zd* LU, int n, int lda, const int* piv, zd* B, int nrhs, int ldb) {
+  if (n <= 0 || nrhs <= 0) return;
+  zlaswp_kernel<<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(B, ldb, nrhs, piv, n);
+  AIFMM_LAUNCHED();
+  // forward: unit lower
+  for (int i0 = 0; i0 < n; i0 += LU_NB) {
+    const int nb = std::min(LU_NB, n - i0);
+    ztrsm_block_kernel<true><<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
+                                                                           B + i0, ldb, nrhs);
+    AIFMM_LAUNCHED();
+    const int rest = n - i0 - nb;
+    if (rest > 0) {
+      GemmProblem g{LU + (size_t)i0 * lda + i0 + nb, B + i0, B + i0 + nb, rest, nrhs, nb, lda, ldb, ldb, OP_N, OP_N,
+                    zmk(-1, 0), zmk(1, 0)};
+      zgemm_grouped(ctx, {g});
+    }
+  }
+  // backward: upper
+  const int last = ((n - 1) / LU_NB) * LU_NB;
+  for (int i0 = last; i0 >= 0; i0 -= LU_NB) {
+    const int nb = std::min(LU_NB, n - i0);
+    ztrsm_block_kernel<false><<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
+                                                                            B + i0, ldb, nrhs);
+    AIFMM_LAUNCHED();
+    if (i0 > 0) {
+      GemmProblem g{LU + (size_t)i0 * lda, B + i0, B, i0, nrhs, nb, lda, ldb, ldb, OP_N, OP_N, zmk(-1, 0),
+                    zmk(1, 0)};
+      zgemm_grouped(ctx, {g});
+    }
+  }
+}
+
+}  // namespace aifmm

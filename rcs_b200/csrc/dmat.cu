@@ -1,0 +1,192 @@
+#include "dmat.cuh"
+
+#include <map>
+
+namespace aifmm {
+
+void GemmBatch::add(DMat& C, const DMat& A, int opA, const DMat& B, int opB, zd alpha, zd beta) {
+  const int m = opA == OP_N ? A.r : A.c;
+  const int k = opA == OP_N ? A.c : A.r;
+  const int kb = opB == OP_N ? B.r : B.c;
+  const int n = opB == OP_N ? B.c : B.r;
+  AIFMM_REQUIRE(k == kb && C.r == m && C.c == n, AIFMM_EINVAL,
+                "GEMM shape mismatch " + std::to_string(m) + "x" + std::to_string(k) + " * " + std::to_string(kb) +
+                    "x" + std::to_string(n) + " -> " + std::to_string(C.r) + "x" + std::to_string(C.c));
+  if (m == 0 || n == 0) return;
+  probs.push_back({A.p, B.p, C.p, m, n, k, A.ld(), B.ld(), C.ld(), opA, opB, alpha, beta});
+}
+
+// Problems that write the same output must not run in one launch (their
+// read-modify-write of C would race): problem q goes to wave w = number of
+// earlier problems with the same C, and waves run in order, which also keeps
+// the accumulation order of each output equal to the insertion order.
+void GemmBatch::flush(aifmm_ctx* ctx) {
+  if (probs.empty()) return;
+  std::map<const zd*, int> seen;
+  std::vector<std::vector<GemmProblem>> waves;
+  for (const GemmProblem& p : probs) {
+    const int w = seen[p.C]++;
+    if ((int)waves.size() <= w) waves.resize(w + 1);
+    waves[w].push_back(p);
+  }
+  for (auto& w : waves) zgemm_grouped(ctx, w);
+  probs.clear();
+}
+
+DMat Ops::alloc(int r, int c) const {
+  AIFMM_REQUIRE(r >= 0 && c >= 0, AIFMM_EINVAL, "negative matrix size");
+  DMat m;
+  m.r = r;
+  m.c = c;
+  if ((long)r * c > 0) {
+    m.buf = std::make_shared<DevBuf>(ctx, sizeof(zd) * (size_t)r * c);
+    m.p = m.buf->as<zd>();
+  }
+  return m;
+}
+DMat Ops::zeros(int r, int c) const {
+  DMat m = alloc(r, c);
+  if (m.size()) AIFMM_CUDA(cudaMemsetAsync(m.p, 0, sizeof(zd) * m.size(), ctx->stream));
+  return m;
+}
+DMat Ops::ident(int n, zd d) const {
+  DMat m = alloc(n, n);
+  if (m.size()) zset_identity(ctx, m.p, n, n, d);
+  return m;
+}
+DMat Ops::copy(const DMat& a) const {
+  DMat m = alloc(a.r, a.c);
+  if (m.size()) AIFMM_CUDA(cudaMemcpyAsync(m.p, a.p, sizeof(zd) * m.size(), cudaMemcpyDeviceToDevice, ctx->stream));
+  return m;
+}
+DMat Ops::block(const DMat& a, int i0, int j0, int nr, int nc) const {
+  AIFMM_REQUIRE(i0 >= 0 && j0 >= 0 && nr >= 0 && nc >= 0 && i0 + nr <= a.r && j0 + nc <= a.c, AIFMM_EINVAL,
+                "block out of range");
+  DMat m = alloc(nr, nc);
+  if (m.size()) zcopy_grouped(ctx, {{a.p + (size_t)j0 * a.ld() + i0, m.p, nr, nc, a.ld(), m.ld(), 0, zmk(1, 0)}});
+  return m;
+}
+DMat Ops::adj(const DMat& a) const {
+  DMat m = alloc(a.c, a.r);
+  if (m.size()) zcopy_grouped(ctx, {{a.p, m.p, a.c, a.r, a.ld(), m.ld(), 1, zmk(1, 0)}});
+  return m;
+}
+DMat Ops::neg(const DMat& a) const {
+  DMat m = alloc(a.r, a.c);
+  if (m.size()) zcopy_grouped(ctx, {{a.p, m.p, a.r, a.c, a.ld(), m.ld(), 0, zmk(-1, 0)}});
+  return m;
+}
+void Ops::setBlock(DMat& dst, int i0, int j0, const DMat& src) const {
+  AIFMM_REQUIRE(i0 >= 0 && j0 >= 0 && i0 + src.r <= dst.r && j0 + src.c <= dst.c, AIFMM_EINVAL,
+                "setBlock out of range");
+  if (src.size()) zcopy_grouped(ctx, {{src.p, dst.p + (size_t)j0 * dst.ld() + i0, src.r, src.c, src.ld(), dst.ld(), 0, zmk(1, 0)}});
+}
+DMat Ops::hcat(const DMat& a, const DMat& b) const { return hcatv({a, b}); }
+DMat Ops::hcatv(const std::vector<DMat>& parts) const {
+  int r = parts.empty() ? 0 : parts[0].r, c = 0;
+  for (const DMat& q : parts) {
+    AIFMM_REQUIRE(q.r == r, AIFMM_EINVAL, "hcat rows mismatch");
+    c += q.c;
+  }
+  DMat m = alloc(r, c);
+  std::vector<CopyProblem> cp;
+  int o = 0;
+  for (const DMat& q : parts) {
+    if (q.size()) cp.push_back({q.p, m.p + (size_t)o * m.ld(), q.r, q.c, q.ld(), m.ld(), 0, zmk(1, 0)});
+    o += q.c;
+  }
+  zcopy_grouped(ctx, cp);
+  return m;
+}
+DMat Ops::vcat(const std::vector<DMat>& parts) const {
+  int r = 0, c = parts.empty() ? 0 : parts[0].c;
+  for (const DMat& q : parts) {
+    AIFMM_REQUIRE(q.c == c, AIFMM_EINVAL, "vcat cols mismatch");
+    r += q.r;
+  }
+  DMat m = alloc(r, c);
+  std::vector<CopyProblem> cp;
+  int o = 0;
+  for (const DMat& q : parts) {
+    if (q.size()) cp.push_back({q.p, m.p + o, q.r, q.c, q.ld(), m.ld(), 0, zmk(1, 0)});
+    o += q.r;
+  }
+  zcopy_grouped(ctx, cp);
+  return m;
+}
+DMat Ops::mul(const DMat& a, int opA, const DMat& b, int opB, zd alpha) const {
+  const int m = opA == OP_N ? a.r : a.c;
+  const int n = opB == OP_N ? b.c : b.r;
+  DMat c = alloc(m, n);
+  const int k = opA == OP_N ? a.c : a.r;
+  if (k == 0) {
+    if (c.size()) AIFMM_CUDA(cudaMemsetAsync(c.p, 0, sizeof(zd) * c.size(), ctx->stream));
+    return c;
+  }
+  GemmBatch g;
+  g.add(c, a, opA, b, opB, alpha, zmk(0, 0));
+  g.flush(ctx);
+  return c;
+}
+std::vector<double> Ops::norms(const std::vector<const DMat*>& ms) const {
+  std::vector<double> out(ms.size(), 0.0);
+  std::vector<NormProblem> ps;
+  std::vector<int> idx;
+  for (size_t i = 0; i < ms.size(); ++i)
+    if (ms[i]->size() > 0) {
+      ps.push_back({ms[i]->p, ms[i]->r, ms[i]->c, ms[i]->ld()});
+      idx.push_back((int)i);
+    }
+  if (ps.empty()) return out;
+  DevBuf d(ctx, sizeof(double) * ps.size());
+  znorm_grouped(ctx, ps, d.as<double>());
+  std::vector<double> h(ps.size());
+  AIFMM_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  for (size_t q = 0; q < idx.size(); ++q) out[idx[q]] = h[q];
+  return out;
+}
+double Ops::maxColNorm(const DMat& a) const {
+  AIFMM_REQUIRE(a.c > 0, AIFMM_EINVAL, "maxColNorm of empty matrix");
+  std::vector<NormProblem> ps;
+  for (int j = 0; j < a.c; ++j) ps.push_back({a.p + (size_t)j * a.ld(), a.r, 1, a.ld()});
+  DevBuf d(ctx, sizeof(double) * ps.size());
+  znorm_grouped(ctx, ps, d.as<double>());
+  std::vector<double> h(ps.size());
+  AIFMM_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  double best = -1.0;
+  for (double v : h) best = std::max(best, v);
+  return best;
+}
+DLU Ops::factor(const DMat& a) const {
+  AIFMM_REQUIRE(a.r == a.c, AIFMM_EINVAL, "LU of a non-square matrix");
+  DLU f;
+  f.n = a.r;
+  f.lu = copy(a);
+  f.piv = std::make_shared<DevBuf>(ctx, sizeof(int) * std::max(1, a.r));
+  f.info = std::make_shared<DevBuf>(ctx, sizeof(int));
+  if (a.r > 0) zgetrf(ctx, f.lu.p, a.r, a.ld(), f.piv->as<int>(), f.info->as<int>());
+  return f;
+}
+DMat Ops::solve(const DLU& f, const DMat& b) const {
+  AIFMM_REQUIRE(b.r == f.n, AIFMM_EINVAL, "LU solve size mismatch");
+  DMat x = copy(b);
+  if (x.size()) zgetrs(ctx, f.lu.p, f.n, f.lu.ld(), f.piv->as<int>(), x.p, x.c, x.ld());
+  return x;
+}
+void Ops::sync() const { AIFMM_CUDA(cudaStreamSynchronize(ctx->stream)); }
+std::vector<zd> Ops::download(const DMat& a) const {
+  std::vector<zd> h((size_t)a.size());
+  if (a.size())
+    AIFMM_CUDA(cudaMemcpyAsync(h.data(), a.p, sizeof(zd) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  sync();
+  return h;
+}
+DMat Ops::fromHost(const std::vector<zd>& v, int r, int c) const {
+  DMat m = alloc(r, c);
+  if (m.size()) AIFMM_CUDA(cudaMemcpyAsync(m.p, v.data(), sizeof(zd) * m.size(), cudaMemcpyHostToDevice, ctx->stream));
+  return m;
+}
+
+}  // namespace aifmm

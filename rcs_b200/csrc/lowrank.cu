@@ -1,0 +1,427 @@
+// ACA and partitioned RRQR kernels.
+//
+// ACA follows LowRank<K>::ACA_only_nodes2 (src/ACA.cpp:639-859): the first
+// pivot is the first primary index whose largest remaining entry exceeds
+// 1e-16; each step evaluates the secondary vector at the primary pivot, takes
+// its largest remaining entry (lowest index on ties, maxAbsVector :25-38),
+// normalises by it, evaluates the primary vector at that pivot, subtracts the
+// previous rank-one terms in order, and updates the reference's normS
+// recurrence (:750-754) -- including the term of the new vector with itself.
+// "Primary" = rows when nr < nc (the reference's first branch), else columns.
+//
+// RRQR follows RRQR::colPivHouseholderQRWithPartition (src/rrqr.cpp:98-182):
+// partition 1 pivots among the old-basis columns with tolerance tol1
+// relative to its first pivot (early exit sets rank_partition1 = j-1, as the
+// reference does), partition 2 pivots among all remaining columns with
+// tolerance tol2 relative to max(inputPivot, its first pivot) and stops after
+// fillInRank columns.  Columns are selected by the largest downdated norm;
+// the reference re-sorts all remaining columns each step, which selects the
+// same column except for exact ties.  Q_trunc is formed by applying the
+// committed reflectors to the first rank columns of the identity, which
+// equals the reference's explicit accumulation of the full Q.
+#include "lowrank.cuh"
+
+namespace aifmm {
+
+// ------------------------------------------------------------------ reductions
+template <int NT>
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffff, v, o);
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) sh[threadIdx.x >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x < 32) {
+    t = (threadIdx.x < NT / 32) ? sh[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffff, t, o);
+    if (threadIdx.x == 0) sh[32] = t;
+  }
+  __syncthreads();
+  return sh[32];
+}
+
+// Largest value, lowest index on ties; idx = -1 when nothing qualifies.
+template <int NT>
+__device__ __forceinline__ void block_argmax(double v, int idx, double* shv, int* shi, double& ov, int& oi) {
+  for (int o = 16; o > 0; o >>= 1) {
+    const double pv = __shfl_xor_sync(0xffffffff, v, o);
+    const int pi = __shfl_xor_sync(0xffffffff, idx, o);
+    if (pi >= 0 && (idx < 0 || pv > v || (pv == v && pi < idx))) { v = pv; idx = pi; }
+  }
+  __syncthreads();
+  if ((threadIdx.x & 31) == 0) { shv[threadIdx.x >> 5] = v; shi[threadIdx.x >> 5] = idx; }
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    v = (threadIdx.x < NT / 32) ? shv[threadIdx.x] : -1.0;
+    idx = (threadIdx.x < NT / 32) ? shi[threadIdx.x] : -1;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double pv = __shfl_xor_sync(0xffffffff, v, o);
+      const int pi = __shfl_xor_sync(0xffffffff, idx, o);
+      if (pi >= 0 && (idx < 0 || pv > v || (pv == v && pi < idx))) { v = pv; idx = pi; }
+    }
+    if (threadIdx.x == 0) { shv[32] = v; shi[32] = idx; }
+  }
+  __syncthreads();
+  ov = shv[32];
+  oi = shi[32];
+}
+
+__device__ __forceinline__ double zabs(zd z) { return hypot(z.x, z.y); }
+
+// ------------------------------------------------------------------ ACA
+constexpr int ACA_NT = 512;
+constexpr int ACA_MAXR = 1024;  // shared dot buffers
+
+template <bool EFIE>
+__device__ __forceinline__ zd kentry(const KernelGeom& kg, int r, int c) {
+  if (EFIE) return efie_entry(kg.ge, r, c);
+  return zmk(es_entry(kg.gs, r, c), 0.0);
+}
+
+template <bool EFIE>
+__global__ void __launch_bounds__(ACA_NT) aca_kernel(KernelGeom kg, const ACAProblem* __restrict__ probs, double tol) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd d1[ACA_MAXR], d2[ACA_MAXR];
+  __shared__ zd s_piv;
+  const ACAProblem P = probs[blockIdx.x];
+  const int tid = threadIdx.x;
+  const bool br1 = P.nr < P.nc;  // primary = rows
+  const int nP = br1 ? P.nr : P.nc, nS = br1 ? P.nc : P.nr;
+  const int* idP = br1 ? P.rows : P.cols;
+  const int* idS = br1 ? P.cols : P.rows;
+  unsigned char* usedP = br1 ? P.used : P.used + P.nr;
+  unsigned char* usedS = br1 ? P.used + P.nr : P.used;
+  const int mn = min(P.nr, P.nc);
+  const int rmax = min(P.rmax, ACA_MAXR);
+  // entry(p, s) in reference orientation
+  auto ent = [&](int p, int s) -> zd { return br1 ? kentry<EFIE>(kg, idP[p], idS[s]) : kentry<EFIE>(kg, idS[s], idP[p]); };
+  // original vectors: the secondary vector is a row of K when br1 (stored in Ar), a column otherwise (Ac)
+  auto origS = [&](int r, int s) -> zd& { return br1 ? P.Ar[(size_t)s * P.rmax + r] : P.Ac[(size_t)r * P.nr + s]; };
+  auto origP = [&](int r, int p) -> zd& { return br1 ? P.Ac[(size_t)r * P.nr + p] : P.Ar[(size_t)p * P.rmax + r]; };
+  zd* U = P.U;  // U[r * nP + p]
+  zd* V = P.V;  // V[r * nS + s]
+  for (int i = tid; i < P.nr + P.nc; i += ACA_NT) P.used[i] = 0;
+  __syncthreads();
+
+  // ---- first pivot (ACA.cpp:670-677 / :761-768)
+  int l, sidx = -1;
+  double mval;
+  for (l = 0; l < nP; ++l) {
+    double bv = -1.0;
+    int bi = -1;
+    for (int s = tid; s < nS; s += ACA_NT) {
+      const zd z = ent(l, s);
+      V[s] = z;
+      origS(0, s) = z;
+      const double a = zabs(z);
+      if (bi < 0 || a > bv) { bv = a; bi = s; }
+    }
+    block_argmax<ACA_NT>(bv, bi, shv, shi, mval, sidx);
+    if (mval > 1e-16) break;
+  }
+  if (l == nP || sidx < 0) {
+    if (tid == 0) { *P.rank = 0; *P.status = 0; }
+    return;
+  }
+  int pidx = l;
+  if (tid == 0) s_piv = V[sidx];
+  __syncthreads();
+  const zd piv0 = s_piv;
+  for (int s = tid; s < nS; s += ACA_NT) V[s] = zdiv(V[s], piv0);
+  for (int p = tid; p < nP; p += ACA_NT) {
+    const zd z = ent(p, sidx);
+    U[p] = z;
+    origP(0, p) = z;
+  }
+  if (tid == 0) {
+    (br1 ? P.rowBases : P.colBases)[0] = pidx;
+    (br1 ? P.colBases : P.rowBases)[0] = sidx;
+    usedP[pidx] = 1;
+    usedS[sidx] = 1;
+  }
+  __syncthreads();
+  int rank = 1;
+  double normS = 0.0;
+  // next primary pivot from u (= the first primary vector)
+  {
+    double bv = -1.0;
+    int bi = -1;
+    for (int p = tid; p < nP; p += ACA_NT)
+      if (!usedP[p]) {
+        const double a = zabs(U[p]);
+        if (bi < 0 || a > bv) { bv = a; bi = p; }
+      }
+    double dummy;
+    block_argmax<ACA_NT>(bv, bi, shv, shi, dummy, pidx);
+  }
+  double un, vn;
+  {
+    double s1 = 0.0, s2 = 0.0;
+    for (int p = tid; p < nP; p += ACA_NT) s1 += zabs2(U[p]);
+    un = sqrt(block_sum<ACA_NT>(s1, shv));
+    for (int s = tid; s < nS; s += ACA_NT) s2 += zabs2(V[s]);
+    vn = sqrt(block_sum<ACA_NT>(s2, shv));
+  }
+  int status = 0;
+  while (un * vn > tol * normS && rank < mn) {
+    if (rank >= rmax || pidx < 0) {
+      status = 1;
+      break;
+    }
+    const int r = rank;
+    zd* Vr = V + (size_t)r * nS;
+    zd* Ur = U + (size_t)r * nP;
+    // secondary residual at the primary pivot
+    double bv = -1.0;
+    int bi = -1;
+    for (int s = tid; s < nS; s += ACA_NT) {
+      zd z = ent(pidx, s);
+      origS(r, s) = z;
+      for (int q = 0; q < r; ++q) z = zsub(z, zmul(U[(size_t)q * nP + pidx], V[(size_t)q * nS + s]));
+      Vr[s] = z;
+      if (!usedS[s]) {
+        const double a = zabs(z);
+        if (bi < 0 || a > bv) { bv = a; bi = s; }
+      }
+    }
+    block_argmax<ACA_NT>(bv, bi, shv, shi, mval, sidx);
+    if (tid == 0) s_piv = Vr[sidx];
+    __syncthreads();
+    const zd piv = s_piv;
+    for (int s = tid; s < nS; s += ACA_NT) Vr[s] = zdiv(Vr[s], piv);
+    // primary residual at the secondary pivot
+    for (int p = tid; p < nP; p += ACA_NT) {
+      zd z = ent(p, sidx);
+      origP(r, p) = z;
+      for (int q = 0; q < r; ++q) z = zsub(z, zmul(V[(size_t)q * nS + sidx], U[(size_t)q * nP + p]));
+      Ur[p] = z;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      (br1 ? P.rowBases : P.colBases)[r] = pidx;
+      (br1 ? P.colBases : P.rowBases)[r] = sidx;
+      usedP[pidx] = 1;
+      usedS[sidx] = 1;
+    }
+    rank = r + 1;
+    // norms and the normS recurrence (ACA.cpp:748-754)
+    {
+      double s1 = 0.0, s2 = 0.0;
+      for (int p = tid; p < nP; p += ACA_NT) s1 += zabs2(Ur[p]);
+      un = sqrt(block_sum<ACA_NT>(s1, shv));
+      for (int s = tid; s < nS; s += ACA_NT) s2 += zabs2(Vr[s]);
+      vn = sqrt(block_sum<ACA_NT>(s2, shv));
+    }
+    const int warp = tid >> 5, lane = tid & 31;
+    for (int q = warp; q < rank; q += ACA_NT / 32) {
+      zd a = zmk(0, 0), b = zmk(0, 0);
+      for (int p = lane; p < nP; p += 32) a = zadd(a, zcmul(U[(size_t)q * nP + p], Ur[p]));
+      for (int s = lane; s < nS; s += 32) b = zadd(b, zcmul(V[(size_t)q * nS + s], Vr[s]));
+      for (int o = 16; o > 0; o >>= 1) {
+        a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+        a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+        b.x += __shfl_xor_sync(0xffffffff, b.x, o);
+        b.y += __shfl_xor_sync(0xffffffff, b.y, o);
+      }
+      if (lane == 0) { d1[q] = a; d2[q] = b; }
+    }
+    __syncthreads();
+    if (tid == 0) {
+      double ns = normS * normS + (un * vn) * (un * vn);
+      for (int q = 0; q < rank; ++q) ns += 2 * zabs(zmul(d1[q], d2[q]));
+      shv[32] = sqrt(ns);
+    }
+    __syncthreads();
+    normS = shv[32];
+    __syncthreads();
+    // next primary pivot from the new primary residual
+    {
+      double pv = -1.0;
+      int pi = -1;
+      for (int p = tid; p < nP; p += ACA_NT)
+        if (!usedP[p]) {
+          const double a = zabs(Ur[p]);
+          if (pi < 0 || a > pv) { pv = a; pi = p; }
+        }
+      double dummy;
+      block_argmax<ACA_NT>(pv, pi, shv, shi, dummy, pidx);
+    }
+  }
+  if (tid == 0) {
+    *P.rank = rank;
+    *P.status = status;
+  }
+}
+
+void launch_aca(aifmm_ctx* ctx, const KernelGeom& k, const std::vector<ACAProblem>& probs, double tol) {
+  if (probs.empty()) return;
+  DevBuf dp = upload(ctx, probs);
+  if (k.efie) aca_kernel<true><<<(unsigned)probs.size(), ACA_NT, 0, ctx->stream>>>(k, dp.as<ACAProblem>(), tol);
+  else aca_kernel<false><<<(unsigned)probs.size(), ACA_NT, 0, ctx->stream>>>(k, dp.as<ACAProblem>(), tol);
+  AIFMM_LAUNCHED();
+}
+
+// ------------------------------------------------------------------ RRQR
+constexpr int QR_NT = 1024;
+
+__global__ void __launch_bounds__(QR_NT) rrqr_kernel(const RRQRProblem* __restrict__ probs) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  const RRQRProblem P = probs[blockIdx.x];
+  const int tid = threadIdx.x, m = P.m, n = P.n;
+  const int warp = tid >> 5, lane = tid & 31, nwarp = QR_NT / 32;
+  zd* R = P.R;
+  // column norms (rrqr.cpp:111) and identity permutation
+  for (int c = warp; c < n; c += nwarp) {
+    double s = 0.0;
+    for (int i = lane; i < m; i += 32) s += zabs2(R[(size_t)c * m + i]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffff, s, o);
+    if (lane == 0) { P.nsq[c] = s; P.perm[c] = c; }
+  }
+  __syncthreads();
+  int nref = 0;  // committed reflectors
+  double maxPivot = 0.0, mp1 = 0.0;
+  const int partition = P.partition;
+  int rank_p1 = min(partition, m);
+  int steps = min(m, n);
+  // One pivoting step at position j over positions [j, end).  Returns false
+  // when the pivot test says stop; the reflector is then not committed.
+  auto step = [&](int j, int end, bool part1, int first) -> bool {
+    // pivot: largest downdated norm among positions [j, end)
+    double bv = -1.0;
+    int bi = -1;
+    for (int q = j + tid; q < end; q += QR_NT) {
+      const double v = P.nsq[q];
+      if (bi < 0 || v > bv) { bv = v; bi = q; }
+    }
+    double mv;
+    int pos;
+    block_argmax<QR_NT>(bv, bi, shv, shi, mv, pos);
+    if (tid == 0 && pos != j) {
+      double t = P.nsq[j]; P.nsq[j] = P.nsq[pos]; P.nsq[pos] = t;
+      int u = P.perm[j]; P.perm[j] = P.perm[pos]; P.perm[pos] = u;
+    }
+    __syncthreads();
+    const int c = P.perm[j];
+    zd* x = R + (size_t)c * m;
+    // Householder vector (gethouselholderVec, rrqr.cpp:75-96)
+    double s = 0.0;
+    for (int i = j + tid; i < m; i += QR_NT) s += zabs2(x[i]);
+    const double xn = sqrt(block_sum<QR_NT>(s, shv));
+    zd* h = P.H + (size_t)nref * m;
+    if (tid == 0) {
+      const zd xj = x[j];
+      zd add;
+      if (P.realMode) add = zmk((xj.x >= 0 ? 1.0 : -1.0) * xn, 0.0);
+      else {
+        double sn, cs;
+        sincos(atan2(xj.y, xj.x), &sn, &cs);
+        add = zmk(cs * xn, sn * xn);
+      }
+      s_alpha = zadd(xj, add);
+    }
+    __syncthreads();
+    double s2 = 0.0;
+    for (int i = tid; i < m; i += QR_NT) {
+      zd v = (i < j) ? zmk(0, 0) : ((i == j) ? s_alpha : x[i]);
+      h[i] = v;
+      s2 += zabs2(v);
+    }
+    const double hn = sqrt(block_sum<QR_NT>(s2, shv));
+    __syncthreads();
+    if (hn > 0) {  // v = v * sqrt(2) / |v|
+      const double r2 = sqrt(2.0);
+      for (int i = j + tid; i < m; i += QR_NT) h[i] = zmk((h[i].x * r2) / hn, (h[i].y * r2) / hn);
+    }
+    __syncthreads();
+    // pivot value after the reflection: R(j,c) - h_j (h^H x)
+    zd w = zmk(0, 0);
+    for (int i = j + tid; i < m; i += QR_NT) w = zadd(w, zcmul(h[i], x[i]));
+    double wr = block_sum<QR_NT>(w.x, shv);
+    double wi = block_sum<QR_NT>(w.y, shv);
+    const zd rjj = zsub(x[j], zmul(h[j], zmk(wr, wi)));
+    const double pivot = zabs(rjj);
+    bool stop;
+    if (part1) {
+      if (j == 0) mp1 = pivot;
+      maxPivot = mp1;
+      stop = (pivot / mp1 < P.tol1);
+    } else {
+      if (j == first) maxPivot = fmax(P.inputPivot, pivot);
+      stop = (pivot / maxPivot < P.tol2 || j - first >= P.fillInRank);
+    }
+    if (stop) return false;
+    // apply the reflector to the columns at positions >= j
+    for (int q = j + warp; q < n; q += nwarp) {
+      zd* y = R + (size_t)P.perm[q] * m;
+      zd a = zmk(0, 0);
+      for (int i = j + lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+      for (int o = 16; o > 0; o >>= 1) {
+        a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+        a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+      }
+      for (int i = j + lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+    }
+    __syncthreads();
+    for (int i = j + 1 + tid; i < m; i += QR_NT) x[i] = zmk(0, 0);
+    for (int q = j + 1 + tid; q < n; q += QR_NT) {
+      const zd rjq = R[(size_t)P.perm[q] * m + j];
+      const double a = zabs(rjq);
+      P.nsq[q] = P.nsq[q] - a * a;
+    }
+    nref++;
+    __syncthreads();
+    return true;
+  };
+  for (int j = 0; j < rank_p1; ++j)
+    if (!step(j, partition, true, 0)) {
+      rank_p1 = j - 1;  // rrqr.cpp:116
+      break;
+    }
+  for (int q = rank_p1 + tid; q < partition; q += QR_NT) P.nsq[q] = 0.0;
+  __syncthreads();
+  steps = steps - (partition - rank_p1);
+  const int first = rank_p1;
+  int rank_p2 = min(steps - first, m);
+  for (int j = first; j < steps; ++j)
+    if (!step(j, n, false, first)) {
+      rank_p2 = j - first;
+      break;
+    }
+  const int rank = rank_p1 + rank_p2;
+  // Q_trunc = H_0 H_1 ... H_{nref-1} [I_rank; 0]
+  for (int t = tid; t < m * rank; t += QR_NT) {
+    const int i = t % m, c = t / m;
+    P.Q[(size_t)c * m + i] = (i == c) ? zmk(1, 0) : zmk(0, 0);
+  }
+  __syncthreads();
+  for (int r = nref - 1; r >= 0; --r) {
+    const zd* h = P.H + (size_t)r * m;
+    for (int c = warp; c < rank; c += nwarp) {
+      zd* y = P.Q + (size_t)c * m;
+      zd a = zmk(0, 0);
+      for (int i = lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+      for (int o = 16; o > 0; o >>= 1) {
+        a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+        a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+      }
+      for (int i = lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+    }
+    __syncthreads();
+  }
+  if (tid == 0) {
+    *P.rank = rank;
+    *P.maxPivot = maxPivot;
+  }
+}
+
+void launch_rrqr(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
+  if (probs.empty()) return;
+  DevBuf dp = upload(ctx, probs);
+  rrqr_kernel<<<(unsigned)probs.size(), QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+  AIFMM_LAUNCHED();
+}
+
+}  // namespace aifmm

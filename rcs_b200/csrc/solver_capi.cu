@@ -1,0 +1,150 @@
+// C ABI of the AIFMM solver (see include/aifmm_b200.h).
+#include <memory>
+
+#include "solver.cuh"
+
+using namespace aifmm;
+
+#define API_BEGIN try {
+#define API_END                               \
+  }                                           \
+  catch (const Error& e) {                    \
+    set_last_error(e.what());                 \
+    return e.code;                            \
+  }                                           \
+  catch (const std::bad_alloc&) {             \
+    set_last_error("host allocation failed"); \
+    return AIFMM_ENOMEM;                      \
+  }                                           \
+  catch (const std::exception& e) {           \
+    set_last_error(e.what());                 \
+    return AIFMM_EINVAL;                      \
+  }                                           \
+  return AIFMM_OK;
+
+extern "C" {
+
+int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && p && out, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(p->precision == 0, AIFMM_ENOTIMPL, "only precision 0 (complex128) is available");
+  AIFMM_REQUIRE(p->leaf_size > 0 && p->tol_pow >= 0 && p->fillin_tol >= 0 && p->n_levels >= 0, AIFMM_EINVAL,
+                "bad solver parameters");
+  SolverParams sp;
+  sp.leafSize = p->leaf_size;
+  sp.tol_pow = p->tol_pow;
+  sp.fillin_tol = p->fillin_tol;
+  sp.fillin_rank = p->fillin_rank;
+  sp.nLevelsInput = p->n_levels;
+  sp.realMode = k->geom.efie ? 0 : 1;
+  std::unique_ptr<aifmm_solver> s(new aifmm_solver);
+  s->s.reset(new Solver(k, sp));
+  s->s->build();
+  ctx_retain(k->ctx);
+  *out = s.release();
+  API_END
+}
+
+int aifmm_solver_factorize(aifmm_solver* s) {
+  API_BEGIN
+  AIFMM_REQUIRE(s, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(!s->s->factored, AIFMM_ESTATE, "already factorized");
+  s->s->factorize();
+  API_END
+}
+
+int aifmm_solver_solve_device(aifmm_solver* s, const void* rhs_device, int nrhs, void* x_device) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && rhs_device && x_device && nrhs > 0, AIFMM_EINVAL, "bad argument");
+  Solver& S = *s->s;
+  AIFMM_CUDA(cudaSetDevice(S.ctx->device));
+  DMat b;
+  b.p = (zd*)rhs_device;  // non-owning view
+  b.r = S.N;
+  b.c = nrhs;
+  DMat x = S.solve(b);
+  AIFMM_CUDA(cudaMemcpyAsync(x_device, x.p, sizeof(zd) * (size_t)S.N * nrhs, cudaMemcpyDeviceToDevice, S.ctx->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
+  API_END
+}
+
+int aifmm_solver_solve(aifmm_solver* s, const double* rhs, int nrhs, double* x) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && rhs && x && nrhs > 0, AIFMM_EINVAL, "bad argument");
+  Solver& S = *s->s;
+  AIFMM_CUDA(cudaSetDevice(S.ctx->device));
+  const size_t bytes = sizeof(zd) * (size_t)S.N * nrhs;
+  DMat b = S.ops.alloc(S.N, nrhs);
+  AIFMM_CUDA(cudaMemcpyAsync(b.p, rhs, bytes, cudaMemcpyHostToDevice, S.ctx->stream));
+  DMat xd = S.solve(b);
+  AIFMM_CUDA(cudaMemcpyAsync(x, xd.p, bytes, cudaMemcpyDeviceToHost, S.ctx->stream));
+  AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
+  API_END
+}
+
+int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && info, AIFMM_EINVAL, "NULL argument");
+  Solver& S = *s->s;
+  info->n = S.N;
+  info->n_levels = S.nLevels;
+  info->start_level = S.startLevel;
+  info->avg_leaf_size = S.avgLeafSize();
+  info->avg_multipoles = S.avgMultipoles();
+  info->max_rank = S.maxRank();
+  info->n_rrqr = S.stats.nRRQR;
+  info->n_compress_p2p = S.stats.nCompressP2P;
+  info->n_compress_p2l = S.stats.nCompressP2L;
+  info->n_aca = S.stats.nACA;
+  info->n_aca_retry = S.stats.nACARetry;
+  info->kernels = S.stats.kernels;
+  info->t_assemble = S.stats.t_assemble;
+  info->t_factor = S.stats.t_factor;
+  info->t_solve = S.stats.t_solve;
+  info->flops_factor = S.stats.flops_factor;
+  info->mem_gb = S.memoryGB(false);
+  info->mem_after_gb = S.memoryGB(true);
+  API_END
+}
+
+int aifmm_solver_checkpoint(aifmm_solver* s) {
+  API_BEGIN
+  AIFMM_REQUIRE(s, AIFMM_EINVAL, "NULL argument");
+  AIFMM_CUDA(cudaSetDevice(s->s->ctx->device));
+  s->s->checkpoint();
+  API_END
+}
+
+int aifmm_solver_rewind(aifmm_solver* s) {
+  API_BEGIN
+  AIFMM_REQUIRE(s, AIFMM_EINVAL, "NULL argument");
+  AIFMM_CUDA(cudaSetDevice(s->s->ctx->device));
+  s->s->rewind();
+  API_END
+}
+
+int aifmm_profile_gemm(int on) {
+  API_BEGIN
+  gemm_profile_enable(on != 0);
+  API_END
+}
+
+int aifmm_profile_gemm_read(double* ms, double* flops, long* launches) {
+  API_BEGIN
+  AIFMM_REQUIRE(ms && flops && launches, AIFMM_EINVAL, "NULL argument");
+  gemm_profile_read(ms, flops, launches);
+  API_END
+}
+
+int aifmm_solver_destroy(aifmm_solver* s) {
+  API_BEGIN
+  if (!s) return AIFMM_OK;
+  aifmm_ctx* c = s->s->ctx;
+  cudaSetDevice(c->device);
+  cudaStreamSynchronize(c->stream);
+  delete s;  // frees every block on the context stream
+  ctx_release(c);
+  API_END
+}
+
+}  // extern "C"

@@ -1,0 +1,137 @@
+"""The AIFMM direct solver on the GPU, with the reference's interface.
+
+``AIFMM`` mirrors vaishna77/RCS include/AIFMM.hpp:11-36: the constructor
+builds the tree, the ACA skeletons, the M2L and leaf P2P blocks
+(src/AIFMM.cpp:7-93); ``factorize`` runs the hierarchical elimination
+(:96-100); ``solve`` = backSubstitute1/2/3 + getPhi (:103-147).  ``A`` exposes
+the tree statistics that the reference's driver prints (getAvgLeafSize,
+getAvgMultipoles, findMemory, findMemoryAfterFactorize, nLevels).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .kernel import kernel
+
+
+class _TreeView:
+    """Read-only stand-in for AIFMM::A (the FMM2DTree) as the driver uses it."""
+
+    def __init__(self, solver: "AIFMM"):
+        self._s = solver
+
+    @property
+    def nLevels(self) -> int:
+        return self._s.info()["n_levels"]
+
+    @property
+    def K(self):
+        return self._s.kernel
+
+    def getAvgLeafSize(self) -> int:
+        return self._s.info()["avg_leaf_size"]
+
+    def getAvgMultipoles(self) -> int:
+        return self._s.info()["avg_multipoles"]
+
+    def findMemory(self) -> float:
+        return self._s.info()["mem_gb"]
+
+    def findMemoryAfterFactorize(self) -> float:
+        return self._s.info()["mem_after_gb"]
+
+
+class AIFMM:
+    def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 8, fillin_tol: int = 10,
+                 fillin_rank: int = 0, n_levels: int = 0, precision: int = 0):
+        p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(fillin_tol), int(fillin_rank), int(n_levels),
+                              int(precision))
+        h = C.c_void_p()
+        _lib.check(_lib.lib().aifmm_solver_create(K.h, C.byref(p), C.byref(h)))
+        self.h = h
+        self.kernel = K
+        self.N = K.N
+        self.A = _TreeView(self)
+        self._rhs = None
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().aifmm_solver_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def factorize(self) -> None:
+        _lib.check(_lib.lib().aifmm_solver_factorize(self.h))
+
+    def solve(self, rhs) -> np.ndarray:
+        """x for one (N,) or several (N, nrhs) right-hand sides."""
+        b = np.asarray(rhs, dtype=np.complex128)
+        one = b.ndim == 1
+        B = b.reshape(self.N, -1)
+        nrhs = B.shape[1]
+        flat = np.ascontiguousarray(B.T).ravel()  # column-major N x nrhs
+        X = np.zeros(self.N * nrhs, dtype=np.complex128)
+        _lib.check(_lib.lib().aifmm_solver_solve(self.h, flat.view(np.float64), nrhs, X.view(np.float64)))
+        Xm = X.reshape(nrhs, self.N).T
+        return Xm[:, 0].copy() if one else Xm.copy()
+
+    def solve_device(self, rhs_ptr: int, nrhs: int, x_ptr: int) -> None:
+        _lib.check(_lib.lib().aifmm_solver_solve_device(self.h, C.c_void_p(rhs_ptr), int(nrhs), C.c_void_p(x_ptr)))
+
+    # the reference's split of solve (src/AIFMM.cpp:120-147)
+    def backSubstitute1(self, rhs) -> None:
+        self._rhs = np.asarray(rhs, dtype=np.complex128)
+
+    def backSubstitute2(self) -> None:
+        pass  # the forward sweep runs inside backSubstitute3 (one device pass)
+
+    def backSubstitute3(self) -> None:
+        self._x = self.solve(self._rhs)
+
+    def getPhi(self) -> np.ndarray:
+        return self._x
+
+    def info(self) -> dict:
+        i = _lib.SolverInfo()
+        _lib.check(_lib.lib().aifmm_solver_get_info(self.h, C.byref(i)))
+        return {f: getattr(i, f) for f, _ in i._fields_}
+
+    def dump(self) -> np.ndarray:
+        """(n, 7) array: level, box, kind, key, rows, cols, Frobenius norm per block."""
+        cnt = C.c_long()
+        _lib.check(_lib.lib().aifmm_solver_dump(self.h, None, 0, C.byref(cnt)))
+        out = np.zeros(7 * cnt.value, dtype=np.float64)
+        _lib.check(_lib.lib().aifmm_solver_dump(self.h, out.ctypes.data, cnt.value, C.byref(cnt)))
+        return out.reshape(-1, 7)
+
+    def checkpoint(self) -> None:
+        """Keep a device copy of the assembled operator (before factorize)."""
+        _lib.check(_lib.lib().aifmm_solver_checkpoint(self.h))
+
+    def rewind(self) -> None:
+        """Restore the checkpointed operator so that factorize can run again."""
+        _lib.check(_lib.lib().aifmm_solver_rewind(self.h))
+
+
+def launch_count() -> int:
+    n = C.c_long()
+    _lib.check(_lib.lib().aifmm_launch_count(C.byref(n)))
+    return n.value
+
+
+def profile_gemm(on: bool) -> None:
+    _lib.check(_lib.lib().aifmm_profile_gemm(int(bool(on))))
+
+
+def profile_gemm_read() -> tuple[float, float, int]:
+    ms, fl, n = C.c_double(), C.c_double(), C.c_long()
+    _lib.check(_lib.lib().aifmm_profile_gemm_read(C.byref(ms), C.byref(fl), C.byref(n)))
+    return ms.value, fl.value, n.value
