@@ -114,6 +114,22 @@ int aifmm_aca(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc,
  * selects the real Householder sign of a USE_DOUBLE build. */
 int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
                double input_pivot, int fill_rank, int real_mode, double* Q, int* rank, double* max_pivot);
+/* The same RRQR for callers that cannot allocate device memory (code running
+ * inside another framework's allocator, during stream capture, or under a
+ * pre-reserved memory budget).  No counterpart in the reference.  Every
+ * argument is a device pointer: A (m x n complex128, column-major, not
+ * modified), Q (m x min(m, n) complex128; its first *rank columns receive
+ * Q_trunc), rank (one int) and max_pivot (one double).  Work is enqueued on
+ * `stream` (a cudaStream_t; NULL = legacy default stream) and is complete when
+ * the stream is.  The call allocates nothing: its working storage is a fixed
+ * 32 MiB device array of the library (held by every GPU that loads it), so
+ * problems with 16 (m n + m (min(m, n) + 1)) + 12 n + 1024 bytes above 32 MiB
+ * are rejected with AIFMM_EOVERFLOW.  The first call on a device looks up that
+ * array's address and must come before any stream capture.  All calls share
+ * the array: calls that overlap on the GPU race. */
+int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int tol_pow1, int tol_pow2,
+                       double input_pivot, int fill_rank, int real_mode, void* Q_device, int* rank_device,
+                       double* max_pivot_device, void* stream);
 /* X = A^{-1} B by partial-pivot LU (Eigen PartialPivLU semantics, as in
  * EFIEMatrix::getCoefficients, src/EFIEMatrix.cpp:831-837). */
 int aifmm_lu_solve(aifmm_ctx* ctx, const double* A, int n, const double* B, int nrhs, double* X);

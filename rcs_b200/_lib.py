@@ -53,6 +53,7 @@ SIGNATURES = {
     "aifmm_launch_count": (_i, [C.POINTER(C.c_long)]),
     "aifmm_aca": (_i, [_p, _ip, _i, _ip, _i, _d, _ip, _ip, C.POINTER(_i), _dp, _dp]),
     "aifmm_rrqr": (_i, [_p, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, C.POINTER(_i), C.POINTER(_d)]),
+    "aifmm_rrqr_noalloc": (_i, [_p, _i, _i, _i, _i, _i, _d, _i, _i, _p, _p, _p, _p]),
     "aifmm_lu_solve": (_i, [_p, _dp, _i, _dp, _i, _dp]),
     "aifmm_solver_dump": (_i, [_p, _p, C.c_long, C.POINTER(C.c_long)]),
     "aifmm_profile_gemm": (_i, [_i]),

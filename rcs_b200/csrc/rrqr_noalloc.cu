@@ -1,0 +1,112 @@
+// aifmm_rrqr_noalloc: the partitioned column-pivoted QR for callers that may
+// not allocate device memory -- code that runs inside another framework's
+// memory manager, on a stream that is being captured into a CUDA graph by a
+// host that forbids allocation during capture, or under a strict memory
+// budget that pre-reserves everything.  Such callers pass device pointers to
+// their own input and outputs; the working storage (the copy of A that the
+// factorization overwrites, the Householder vectors, the column norms and the
+// permutation) lives in the fixed-size device array below, which every GPU
+// that loads this library keeps until the process exits.
+//
+// Set-up: the first call on a device, with that device current, looks up the
+// array's device address with cudaGetSymbolAddress (the name of a
+// __device__ array is only a host-side stand-in, not a device address) and
+// caches it.  Make that first call before any stream capture.
+//
+// All calls share the one array: calls whose work overlaps on the GPU (two
+// streams, or two host threads) race and corrupt each other.  Serialise them,
+// e.g. on one stream.
+#include <algorithm>
+#include <cmath>
+#include <mutex>
+
+#include "lowrank.cuh"
+
+namespace aifmm {
+
+// Defined in lowrank.cu; launched unchanged with 1024 threads per block.
+__global__ void rrqr_kernel(const RRQRProblem* __restrict__ probs);
+constexpr int kRRQRThreads = 1024;
+
+// 32 MiB of scratch: enough for an m x n problem with
+// 16 (m n + m (min(m, n) + 1)) + 12 n + 1 KiB <= 32 MiB, e.g. 1000 x 1000.
+constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
+static __device__ __align__(256) unsigned char g_rrqr_scratch[kNoAllocScratchBytes];
+
+static std::mutex g_scratch_mu;
+static void* g_scratch_addr[128] = {nullptr};
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+__global__ void rrqr_noalloc_setup_kernel(RRQRProblem P, RRQRProblem* dst, const zd* A) {
+  if (blockIdx.x == 0 && threadIdx.x == 0) *dst = P;
+  const size_t n = (size_t)P.m * P.n;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x)
+    P.R[i] = A[i];
+}
+
+}  // namespace aifmm
+
+using namespace aifmm;
+
+extern "C" int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int tol_pow1, int tol_pow2,
+                                  double input_pivot, int fill_rank, int real_mode, void* Q_device,
+                                  int* rank_device, double* max_pivot_device, void* stream) {
+  try {
+    AIFMM_REQUIRE(A_device && Q_device && rank_device && max_pivot_device, AIFMM_EINVAL, "NULL argument");
+    AIFMM_REQUIRE(m > 0 && n > 0 && partition >= 0 && partition <= n, AIFMM_EINVAL, "bad sizes");
+    const size_t hs = (size_t)std::min(m, n) + 1;
+    const size_t off_R = 1024;
+    const size_t off_H = align256(off_R + sizeof(zd) * (size_t)m * n);
+    const size_t off_nsq = align256(off_H + sizeof(zd) * (size_t)m * hs);
+    const size_t off_perm = align256(off_nsq + sizeof(double) * (size_t)n);
+    const size_t need = off_perm + sizeof(int) * (size_t)n;
+    AIFMM_REQUIRE(need <= kNoAllocScratchBytes, AIFMM_EOVERFLOW,
+                  "problem needs " + std::to_string(need) + " bytes of scratch; the fixed scratch array holds " +
+                      std::to_string(kNoAllocScratchBytes));
+    int dev = 0;
+    AIFMM_CUDA(cudaGetDevice(&dev));
+    AIFMM_REQUIRE(dev >= 0 && dev < 128, AIFMM_EINVAL, "device index out of range");
+    void* base = nullptr;
+    {
+      std::lock_guard<std::mutex> l(g_scratch_mu);
+      if (!g_scratch_addr[dev]) {
+        void* p = nullptr;
+        AIFMM_CUDA(cudaGetSymbolAddress(&p, g_rrqr_scratch));  // with this device current
+        g_scratch_addr[dev] = p;
+      }
+      base = g_scratch_addr[dev];
+    }
+    unsigned char* b = static_cast<unsigned char*>(base);
+    RRQRProblem P;
+    P.R = reinterpret_cast<zd*>(b + off_R);
+    P.m = m;
+    P.n = n;
+    P.partition = partition;
+    P.tol1 = std::pow(10.0, -tol_pow1);
+    P.tol2 = std::pow(10.0, -tol_pow2);
+    P.inputPivot = input_pivot;
+    P.fillInRank = fill_rank;
+    P.realMode = real_mode;
+    P.H = reinterpret_cast<zd*>(b + off_H);
+    P.nsq = reinterpret_cast<double*>(b + off_nsq);
+    P.perm = reinterpret_cast<int*>(b + off_perm);
+    P.Q = static_cast<zd*>(Q_device);
+    P.rank = rank_device;
+    P.maxPivot = max_pivot_device;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    RRQRProblem* desc = reinterpret_cast<RRQRProblem*>(b);
+    const int grid = (int)std::min<size_t>(((size_t)m * n + 255) / 256, 148 * 4);
+    rrqr_noalloc_setup_kernel<<<std::max(grid, 1), 256, 0, s>>>(P, desc, static_cast<const zd*>(A_device));
+    AIFMM_LAUNCHED();
+    rrqr_kernel<<<1, kRRQRThreads, 0, s>>>(desc);
+    AIFMM_LAUNCHED();
+  } catch (const Error& e) {
+    set_last_error(e.what());
+    return e.code;
+  } catch (const std::exception& e) {
+    set_last_error(e.what());
+    return AIFMM_EINVAL;
+  }
+  return AIFMM_OK;
+}
