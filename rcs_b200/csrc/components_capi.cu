@@ -88,10 +88,11 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
   API_BEGIN
   AIFMM_REQUIRE(ctx && A && Q && rank && max_pivot, AIFMM_EINVAL, "NULL argument");
   AIFMM_REQUIRE(m > 0 && n > 0 && partition >= 0 && partition <= n, AIFMM_EINVAL, "bad sizes");
+  AIFMM_REQUIRE(tol_pow1 >= 0 && tol_pow2 >= 0 && fill_rank >= 0, AIFMM_EINVAL, "negative tolerance power or fill-in rank");
   AIFMM_CUDA(cudaSetDevice(ctx->device));
   const int hs = std::min(m, n) + 1;
   DevBuf R(ctx, sizeof(zd) * (size_t)m * n), H(ctx, sizeof(zd) * (size_t)m * hs), Qd(ctx, sizeof(zd) * (size_t)m * hs);
-  DevBuf nsq(ctx, sizeof(double) * n), perm(ctx, sizeof(int) * n), out(ctx, 16);
+  DevBuf nsq(ctx, sizeof(double) * n), perm(ctx, sizeof(int) * n), out(ctx, 64);
   AIFMM_CUDA(cudaMemcpyAsync(R.p, A, sizeof(zd) * (size_t)m * n, cudaMemcpyHostToDevice, ctx->stream));
   RRQRProblem P;
   P.R = R.as<zd>();
@@ -109,7 +110,9 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
   P.Q = Qd.as<zd>();
   P.rank = out.as<int>();
   P.maxPivot = (double*)((char*)out.p + 8);
-  launch_rrqr(ctx, {P});
+  P.istate = (int*)((char*)out.p + 16);
+  P.dstate = (double*)((char*)out.p + 32);
+  launch_rrqr_split(ctx, {P});
   struct {
     int r, pad;
     double mp;

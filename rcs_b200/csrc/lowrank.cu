@@ -425,3 +425,235 @@ void launch_rrqr(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
 }
 
 }  // namespace aifmm
+
+// ------------------------------------------------------------------ RRQR, split
+namespace aifmm {
+
+// One pivoting step at position j: pivot among positions [j, end), reflector
+// applied to (and norms downdated for) positions [j, applyEnd).  Same
+// arithmetic as the step of rrqr_kernel.  Returns false on the stop test.
+__device__ bool rrqr_step_dev(const RRQRProblem& P, int j, int end, int applyEnd, bool part1, int first, int& nref,
+                              double& mp1, double& maxPivot, double* shv, int* shi, zd& s_alpha) {
+  const int tid = threadIdx.x, m = P.m;
+  const int warp = tid >> 5, lane = tid & 31, nwarp = QR_NT / 32;
+  zd* R = P.R;
+  double bv = -1.0;
+  int bi = -1;
+  for (int q = j + tid; q < end; q += QR_NT) {
+    const double v = P.nsq[q];
+    if (bi < 0 || v > bv) { bv = v; bi = q; }
+  }
+  double mv;
+  int pos;
+  block_argmax<QR_NT>(bv, bi, shv, shi, mv, pos);
+  if (tid == 0 && pos != j) {
+    double t = P.nsq[j]; P.nsq[j] = P.nsq[pos]; P.nsq[pos] = t;
+    int u = P.perm[j]; P.perm[j] = P.perm[pos]; P.perm[pos] = u;
+  }
+  __syncthreads();
+  const int c = P.perm[j];
+  zd* x = R + (size_t)c * m;
+  double s = 0.0;
+  for (int i = j + tid; i < m; i += QR_NT) s += zabs2(x[i]);
+  const double xn = sqrt(block_sum<QR_NT>(s, shv));
+  zd* h = P.H + (size_t)nref * m;
+  if (tid == 0) {
+    const zd xj = x[j];
+    zd add;
+    if (P.realMode) add = zmk((xj.x >= 0 ? 1.0 : -1.0) * xn, 0.0);
+    else {
+      double sn, cs;
+      sincos(atan2(xj.y, xj.x), &sn, &cs);
+      add = zmk(cs * xn, sn * xn);
+    }
+    s_alpha = zadd(xj, add);
+  }
+  __syncthreads();
+  double s2 = 0.0;
+  for (int i = tid; i < m; i += QR_NT) {
+    zd v = (i < j) ? zmk(0, 0) : ((i == j) ? s_alpha : x[i]);
+    h[i] = v;
+    s2 += zabs2(v);
+  }
+  const double hn = sqrt(block_sum<QR_NT>(s2, shv));
+  __syncthreads();
+  if (hn > 0) {
+    const double r2 = sqrt(2.0);
+    for (int i = j + tid; i < m; i += QR_NT) h[i] = zmk((h[i].x * r2) / hn, (h[i].y * r2) / hn);
+  }
+  __syncthreads();
+  zd w = zmk(0, 0);
+  for (int i = j + tid; i < m; i += QR_NT) w = zadd(w, zcmul(h[i], x[i]));
+  double wr = block_sum<QR_NT>(w.x, shv);
+  double wi = block_sum<QR_NT>(w.y, shv);
+  const zd rjj = zsub(x[j], zmul(h[j], zmk(wr, wi)));
+  const double pivot = zabs(rjj);
+  bool stop;
+  if (part1) {
+    if (j == 0) mp1 = pivot;
+    maxPivot = mp1;
+    stop = (pivot / mp1 < P.tol1);
+  } else {
+    if (j == first) maxPivot = fmax(P.inputPivot, pivot);
+    stop = (pivot / maxPivot < P.tol2 || j - first >= P.fillInRank);
+  }
+  if (stop) return false;
+  for (int q = j + warp; q < applyEnd; q += nwarp) {
+    zd* y = R + (size_t)P.perm[q] * m;
+    zd a = zmk(0, 0);
+    for (int i = j + lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+    for (int o = 16; o > 0; o >>= 1) {
+      a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+      a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+    }
+    for (int i = j + lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+  }
+  __syncthreads();
+  for (int i = j + 1 + tid; i < m; i += QR_NT) x[i] = zmk(0, 0);
+  for (int q = j + 1 + tid; q < applyEnd; q += QR_NT) {
+    const zd rjq = R[(size_t)P.perm[q] * m + j];
+    const double a = zabs(rjq);
+    P.nsq[q] = P.nsq[q] - a * a;
+  }
+  nref++;
+  __syncthreads();
+  return true;
+}
+
+// Partition 1 on the old-basis panel (positions [0, partition)).
+__global__ void __launch_bounds__(QR_NT) rrqr_p1_kernel(const RRQRProblem* __restrict__ probs) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  const RRQRProblem P = probs[blockIdx.x];
+  const int tid = threadIdx.x, m = P.m, n = P.n;
+  const int warp = tid >> 5, lane = tid & 31, nwarp = QR_NT / 32;
+  for (int q = tid; q < n; q += QR_NT) P.perm[q] = q;
+  for (int c = warp; c < P.partition; c += nwarp) {
+    double s = 0.0;
+    for (int i = lane; i < m; i += 32) s += zabs2(P.R[(size_t)c * m + i]);
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffff, s, o);
+    if (lane == 0) P.nsq[c] = s;
+  }
+  __syncthreads();
+  int nref = 0;
+  double mp1 = 0.0, maxPivot = 0.0;
+  int rank_p1 = min(P.partition, m);
+  for (int j = 0; j < rank_p1; ++j)
+    if (!rrqr_step_dev(P, j, P.partition, P.partition, true, 0, nref, mp1, maxPivot, shv, shi, s_alpha)) {
+      rank_p1 = j - 1;
+      break;
+    }
+  if (tid == 0) {
+    P.istate[0] = nref;
+    P.istate[1] = rank_p1;
+    P.dstate[0] = mp1;
+    P.dstate[1] = maxPivot;
+  }
+}
+
+// The committed partition-1 reflectors applied to every fill-in column (one
+// warp per column), with the reference's norm downdates in step order.
+__global__ void rrqr_fill_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int m = P.m;
+  const int lane = threadIdx.x & 31;
+  const int q = P.partition + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= P.n) return;
+  const int nref = P.istate[0];
+  zd* y = P.R + (size_t)q * m;
+  double s = 0.0;
+  for (int i = lane; i < m; i += 32) s += zabs2(y[i]);
+  for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffff, s, o);
+  double nsq = s;
+  for (int r = 0; r < nref; ++r) {
+    const zd* h = P.H + (size_t)r * m;
+    zd a = zmk(0, 0);
+    for (int i = r + lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+    for (int o = 16; o > 0; o >>= 1) {
+      a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+      a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+    }
+    for (int i = r + lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+    __syncwarp();
+    const double ab = zabs(y[r]);
+    nsq = nsq - ab * ab;
+  }
+  if (lane == 0) P.nsq[q] = nsq;
+}
+
+// Partition 2 over positions [first, n), then the rank and outputs.
+__global__ void __launch_bounds__(QR_NT) rrqr_p2_kernel(const RRQRProblem* __restrict__ probs) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  const RRQRProblem P = probs[blockIdx.x];
+  const int tid = threadIdx.x, m = P.m, n = P.n;
+  int nref = P.istate[0];
+  int rank_p1 = P.istate[1];
+  double mp1 = P.dstate[0], maxPivot = P.dstate[1];
+  const int partition = P.partition;
+  for (int q = rank_p1 + tid; q < partition; q += QR_NT) P.nsq[q] = 0.0;
+  __syncthreads();
+  const int steps = min(m, n) - (partition - rank_p1);
+  const int first = rank_p1;
+  int rank_p2 = min(steps - first, m);
+  for (int j = first; j < steps; ++j)
+    if (!rrqr_step_dev(P, j, n, n, false, first, nref, mp1, maxPivot, shv, shi, s_alpha)) {
+      rank_p2 = j - first;
+      break;
+    }
+  if (tid == 0) {
+    P.istate[2] = nref;
+    P.istate[3] = rank_p1 + rank_p2;
+    *P.rank = rank_p1 + rank_p2;
+    *P.maxPivot = maxPivot;
+  }
+}
+
+// Q_trunc column c = H_0 ... H_{nref-1} e_c, one warp per column.
+__global__ void rrqr_q_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int m = P.m;
+  const int lane = threadIdx.x & 31;
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  const int nref = P.istate[2], rank = P.istate[3];
+  if (c >= rank) return;
+  zd* y = P.Q + (size_t)c * m;
+  for (int i = lane; i < m; i += 32) y[i] = (i == c) ? zmk(1, 0) : zmk(0, 0);
+  __syncwarp();
+  for (int r = nref - 1; r >= 0; --r) {
+    const zd* h = P.H + (size_t)r * m;
+    zd a = zmk(0, 0);
+    for (int i = lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+    for (int o = 16; o > 0; o >>= 1) {
+      a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+      a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+    }
+    for (int i = lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+    __syncwarp();
+  }
+}
+
+void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
+  if (probs.empty()) return;
+  int maxFill = 1, maxCols = 1;
+  for (const RRQRProblem& p : probs) {
+    AIFMM_REQUIRE(p.istate && p.dstate, AIFMM_EINVAL, "split RRQR needs istate/dstate");
+    maxFill = std::max(maxFill, p.n - p.partition);
+    maxCols = std::max(maxCols, std::min(p.m, p.n));
+  }
+  AIFMM_REQUIRE(probs.size() <= 65535, AIFMM_EINVAL, "too many RRQR problems in one launch");
+  DevBuf dp = upload(ctx, probs);
+  const unsigned np = (unsigned)probs.size();
+  rrqr_p1_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+  AIFMM_LAUNCHED();
+  rrqr_fill_kernel<<<dim3((maxFill + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+  AIFMM_LAUNCHED();
+  rrqr_p2_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+  AIFMM_LAUNCHED();
+  rrqr_q_kernel<<<dim3((maxCols + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+  AIFMM_LAUNCHED();
+}
+
+}  // namespace aifmm

@@ -41,8 +41,16 @@ struct RRQRProblem {
   zd* Q;             // out: m x rank (ld = m), space for m x (min(m,n)+1)
   int* rank;         // out
   double* maxPivot;  // out
+  int* istate;       // split pipeline only: 4 ints of scratch
+  double* dstate;    // split pipeline only: 2 doubles of scratch
 };
 
+// Single-kernel RRQR (one CTA per problem).
 void launch_rrqr(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs);
+// Same factorization in four launches: the partition-1 panel in one CTA,
+// the committed reflectors applied to the fill-in columns one warp per
+// column, the partition-2 steps in one CTA, and Q_trunc one warp per column.
+// Needs istate/dstate; the result equals launch_rrqr's bit for bit.
+void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs);
 
 }  // namespace aifmm

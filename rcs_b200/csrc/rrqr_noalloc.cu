@@ -55,6 +55,8 @@ extern "C" int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partit
   try {
     AIFMM_REQUIRE(A_device && Q_device && rank_device && max_pivot_device, AIFMM_EINVAL, "NULL argument");
     AIFMM_REQUIRE(m > 0 && n > 0 && partition >= 0 && partition <= n, AIFMM_EINVAL, "bad sizes");
+    AIFMM_REQUIRE(tol_pow1 >= 0 && tol_pow2 >= 0 && fill_rank >= 0, AIFMM_EINVAL,
+                  "negative tolerance power or fill-in rank");
     const size_t hs = (size_t)std::min(m, n) + 1;
     const size_t off_R = 1024;
     const size_t off_H = align256(off_R + sizeof(zd) * (size_t)m * n);
@@ -94,6 +96,8 @@ extern "C" int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partit
     P.Q = static_cast<zd*>(Q_device);
     P.rank = rank_device;
     P.maxPivot = max_pivot_device;
+    P.istate = nullptr;  // the single-kernel form keeps its state in registers
+    P.dstate = nullptr;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     RRQRProblem* desc = reinterpret_cast<RRQRProblem*>(b);
     const int grid = (int)std::min<size_t>(((size_t)m * n + 255) / 256, 148 * 4);

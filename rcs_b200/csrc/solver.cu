@@ -518,8 +518,10 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
   P.Q = Q.as<zd>();
   P.rank = (int*)out.p;
   P.maxPivot = (double*)((char*)out.p + 8);
-  launch_rrqr(ctx, {P});
-  stats.kernels++;
+  P.istate = (int*)((char*)out.p + 16);
+  P.dstate = (double*)((char*)out.p + 32);
+  launch_rrqr_split(ctx, {P});
+  stats.kernels += 4;
   stats.nRRQR++;
   struct {
     int rank, pad;

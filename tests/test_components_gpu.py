@@ -61,6 +61,40 @@ def test_rrqr_matches_oracle(seed, m, r0, nf, frank, tp1, tp2, fr, ip):
         assert rel(Q, Qo) < 1e-10
 
 
+def _single_kernel_rrqr(A, tp1, tp2, part, pivot, fill):
+    """The one-CTA RRQR kernel, reached through the allocation-free entry point."""
+    import ctypes as C
+    import torch
+    from rcs_b200 import _lib
+    m, n = A.shape
+    Ad = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    Qd = torch.zeros((min(m, n) + 1, m), dtype=torch.complex128, device="cuda")
+    rk = torch.zeros(1, dtype=torch.int32, device="cuda")
+    mp = torch.zeros(1, dtype=torch.float64, device="cuda")
+    _lib.check(_lib.lib().aifmm_rrqr_noalloc(C.c_void_p(Ad.data_ptr()), m, n, part, tp1, tp2, float(pivot), fill, 0,
+                                             C.c_void_p(Qd.data_ptr()), C.c_void_p(rk.data_ptr()),
+                                             C.c_void_p(mp.data_ptr()), None))
+    torch.cuda.synchronize()
+    r = int(rk.item())
+    return Qd.cpu().numpy()[:r].T, float(mp.item())
+
+
+@pytest.mark.parametrize("seed,m,r0,nf,frank,tp1,tp2,fr,ip", [
+    (2, 60, 10, 30, 8, 8, 10, 5, 10.0),
+    (3, 25, 12, 40, 20, 6, 8, 10, 0.5),
+    (4, 50, 0, 20, 7, 8, 9, 10, 2.0),
+    (5, 300, 90, 1200, 60, 7, 9, 10, 1.0),   # fill-in recompression shape of a 128-unknown leaf level
+    (6, 200, 200, 0, 1, 7, 9, 5, 1.0),       # no fill-in columns
+])
+def test_rrqr_split_pipeline_bit_exact(seed, m, r0, nf, frank, tp1, tp2, fr, ip):
+    """The four-launch RRQR used by the solver equals the one-CTA kernel bit for bit."""
+    A = _rrqr_case(seed, m, r0, nf, frank) if nf else _rrqr_case(seed, m, r0, 1, 1)[:, :r0]
+    Q1, mp1 = _single_kernel_rrqr(A, tp1, tp2, r0, ip, fr)
+    Q4, mp4 = lowrank.RRQR(A, tp1, tp2, r0, ip, fr)
+    assert Q1.shape == Q4.shape and mp1 == mp4
+    assert np.array_equal(Q1, Q4)
+
+
 def test_lu_solve():
     rng = np.random.default_rng(0)
     for n in (1, 31, 32, 33, 200, 517):
