@@ -150,6 +150,12 @@ typedef struct {
   double t_assemble, t_factor, t_solve; /* seconds, wall clock on the host thread */
   double flops_factor;                  /* algorithmic flops of the factorization (complex counted) */
   double mem_gb, mem_after_gb;          /* findMemory / findMemoryAfterFactorize */
+  /* Factorization phase seconds: RRQR calls, fill-in recompressions (RRQR
+   * included), eliminate_x, eliminate_z, non-leaf P2P assembly.  Exact when the
+   * environment variable AIFMM_PHASE_TIMES=1 was set at solver creation (the
+   * solver then synchronises at every phase boundary), else host-side
+   * approximations. */
+  double t_rrqr, t_compress, t_elim_x, t_elim_z, t_nonleaf;
 } aifmm_solver_info;
 
 /* AIFMM<K>::AIFMM(inputsToSolverClass, K*) (src/AIFMM.cpp:7-93): builds the
@@ -179,6 +185,41 @@ int aifmm_solver_rewind(aifmm_solver* s);
  * 0 L2P, 1 P2M, 2 M2L, 3 P2P, 4 M2P, 5 P2L, 6 L2P_f, 7 P2M_f, 8 M2M_f, 9 L2M_f.
  * Writes at most cap records; *count receives the total. */
 int aifmm_solver_dump(aifmm_solver* s, double* out, long cap, long* count);
+
+/* ---- forward operator and FP64 refinement ----------------------------------- */
+/* No counterpart in the reference, which factorizes its tree directly and
+ * measures the backward error with a dense product (test/sphere.cpp:331-338).
+ * The H^2 forward operator y = A x of the kernel: the assembly of
+ * aifmm_solver_create (octree, ACA skeletons, L2P/P2M, M2L, leaf P2P) run with
+ * p->tol_pow as the operator's ACA tolerance and kept unfactorized; applied
+ * upward (P2M), across (M2L) and downward (L2P) plus the leaf near field.  Used
+ * as the residual operator of aifmm_solver_solve_gmres, so its tolerance should
+ * be tighter than the factorization's. */
+typedef struct aifmm_operator aifmm_operator;
+int aifmm_operator_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_operator** out);
+/* y = A x, n x nrhs column-major complex host arrays. */
+int aifmm_operator_apply(aifmm_operator* op, const double* x, int nrhs, double* y);
+/* Same with device pointers (complex128, n x nrhs, ld = n). */
+int aifmm_operator_apply_device(aifmm_operator* op, const void* x_device, int nrhs, void* y_device);
+/* Device bytes of the operator's blocks and complex-counted flops of one column. */
+int aifmm_operator_info(aifmm_operator* op, double* bytes, double* flops_per_column);
+int aifmm_operator_destroy(aifmm_operator* op);
+
+typedef struct {
+  int iterations;    /* Arnoldi steps: one preconditioner solve and one product each */
+  int cycles;        /* restarts + 1 */
+  double relres;     /* max over columns of ||b - A x|| / ||b||, A = the operator */
+  double t_precond;  /* seconds in preconditioner solves */
+  double t_matvec;   /* seconds in operator products */
+} aifmm_gmres_info;
+/* Flexible GMRES(restart) for A x = b, right-preconditioned by the factorized
+ * solver s (its solve sweeps), until relres <= tol or maxit Arnoldi steps.
+ * s and A must come from the same context and kernel. */
+int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* rhs, int nrhs, double* x, double tol,
+                             int restart, int maxit, aifmm_gmres_info* info);
+/* Same with device pointers (complex128, n x nrhs, ld = n). */
+int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const void* rhs_device, int nrhs,
+                                    void* x_device, double tol, int restart, int maxit, aifmm_gmres_info* info);
 
 /* Number of CUDA kernels this library has launched in the process. */
 int aifmm_launch_count(long* n);

@@ -56,6 +56,13 @@ SIGNATURES = {
     "aifmm_rrqr_noalloc": (_i, [_p, _i, _i, _i, _i, _i, _d, _i, _i, _p, _p, _p, _p]),
     "aifmm_lu_solve": (_i, [_p, _dp, _i, _dp, _i, _dp]),
     "aifmm_solver_dump": (_i, [_p, _p, C.c_long, C.POINTER(C.c_long)]),
+    "aifmm_operator_create": (_i, [_p, _p, _pp]),
+    "aifmm_operator_apply": (_i, [_p, _dp, _i, _dp]),
+    "aifmm_operator_apply_device": (_i, [_p, _p, _i, _p]),
+    "aifmm_operator_info": (_i, [_p, C.POINTER(_d), C.POINTER(_d)]),
+    "aifmm_operator_destroy": (_i, [_p]),
+    "aifmm_solver_solve_gmres": (_i, [_p, _p, _dp, _i, _dp, _d, _i, _i, _p]),
+    "aifmm_solver_solve_gmres_device": (_i, [_p, _p, _p, _i, _p, _d, _i, _i, _p]),
     "aifmm_profile_gemm": (_i, [_i]),
     "aifmm_profile_gemm_read": (_i, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_long)]),
 }
@@ -72,7 +79,14 @@ class SolverInfo(C.Structure):
                 ("n_compress_p2p", C.c_long), ("n_compress_p2l", C.c_long), ("n_aca", C.c_long),
                 ("n_aca_retry", C.c_long), ("kernels", C.c_long), ("t_assemble", C.c_double),
                 ("t_factor", C.c_double), ("t_solve", C.c_double), ("flops_factor", C.c_double),
-                ("mem_gb", C.c_double), ("mem_after_gb", C.c_double)]
+                ("mem_gb", C.c_double), ("mem_after_gb", C.c_double), ("t_rrqr", C.c_double),
+                ("t_compress", C.c_double), ("t_elim_x", C.c_double), ("t_elim_z", C.c_double),
+                ("t_nonleaf", C.c_double)]
+
+class GmresInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("cycles", C.c_int), ("relres", C.c_double), ("t_precond", C.c_double),
+                ("t_matvec", C.c_double)]
+
 
 _lib = None
 

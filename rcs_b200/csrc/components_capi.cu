@@ -2,26 +2,11 @@
 #include <array>
 #include <cstring>
 
+#include "capi_guard.cuh"
 #include "solver.cuh"
 
 using namespace aifmm;
 
-#define API_BEGIN try {
-#define API_END                               \
-  }                                           \
-  catch (const Error& e) {                    \
-    set_last_error(e.what());                 \
-    return e.code;                            \
-  }                                           \
-  catch (const std::bad_alloc&) {             \
-    set_last_error("host allocation failed"); \
-    return AIFMM_ENOMEM;                      \
-  }                                           \
-  catch (const std::exception& e) {           \
-    set_last_error(e.what());                 \
-    return AIFMM_EINVAL;                      \
-  }                                           \
-  return AIFMM_OK;
 
 extern "C" {
 

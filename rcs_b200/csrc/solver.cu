@@ -13,6 +13,23 @@ static double wall() {
 }
 static const zd ONE = {1.0, 0.0}, ZERO = {0.0, 0.0}, MONE = {-1.0, 0.0};
 
+// Adds the wall time of a scope to a phase counter; with phaseTiming the
+// stream is drained on entry and exit so the time is the phase's own.
+// Nested scopes (RRQR inside a recompression) count in both.
+struct PhaseTimer {
+  Solver& s;
+  double& acc;
+  double t0;
+  PhaseTimer(Solver& so, double& a) : s(so), acc(a) {
+    if (s.prm.phaseTiming) s.ops.sync();
+    t0 = wall();
+  }
+  ~PhaseTimer() {
+    if (s.prm.phaseTiming) cudaStreamSynchronize(s.ctx->stream);
+    acc += wall() - t0;
+  }
+};
+
 // ------------------------------------------------------------ setup, T:52-165
 Solver::Solver(aifmm_kernel* k, const SolverParams& p) : K(k), ctx(k->ctx), ops(k->ctx), prm(p) {
   N = k->geom.N;
@@ -420,6 +437,7 @@ void Solver::build() {  // AIFMM.cpp:7-93
 
 // ------------------------------------------------------------ non-leaf P2P, T:3413-3504
 void Solver::initP2PNonLeaf(int j) {
+  PhaseTimer pt(*this, stats.t_nonleaf);
   std::vector<CopyProblem> cps;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
     DBox& B = tree[j][k];
@@ -497,6 +515,7 @@ bool Solver::wellSeparated(int j, int k, int l) const {  // T:4044-4055
 }
 
 DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot) {
+  PhaseTimer pt(*this, stats.t_rrqr);
   const int m = A.r, n = A.c;
   const int hs = std::min(m, n) + 1;
   DMat R = ops.copy(A);
@@ -639,6 +658,7 @@ static void equalise(Ops& ops, const DMat& L2P, const DMat& P2Mt, DMat& L2Pm, DM
 
 void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   if (tree[j][b].M2L[k].size() == 0 || tree[j][k].M2L[b].size() == 0) return;
+  PhaseTimer pt(*this, stats.t_compress);
   stats.nCompressP2P++;
   DMat nL2P_k, nP2Mt_b, M2L_k_b, nL2P_b, nP2Mt_k, M2L_b_k;
   {
@@ -678,6 +698,7 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
 
 void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   if (tree[j][b].M2L[k].size() == 0 || tree[j][k].M2L[b].size() == 0) return;
+  PhaseTimer pt(*this, stats.t_compress);
   stats.nCompressP2L++;
   DBox& Bk = tree[j][k];
   // compress_M2P_myRRQR(j, k, b)
@@ -722,6 +743,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
 // ------------------------------------------------------------ elimination
 // eliminate_x, T:3561-3611 with :3656-3791 (empty box) and :3800-4042.
 void Solver::eliminateX(int j, int k) {
+  PhaseTimer pt(*this, stats.t_elim_x);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;
@@ -831,6 +853,7 @@ void Solver::eliminateX(int j, int k) {
 
 // eliminate_z, T:4081-4113 with :4151-4296 (empty) and :4304-4509.
 void Solver::eliminateZ(int j, int k) {
+  PhaseTimer pt(*this, stats.t_elim_z);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;
@@ -956,6 +979,7 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   AIFMM_CUDA(cudaSetDevice(ctx->device));
   stats.nRRQR = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
+  stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
   for (int j = nLevels; j >= startLevel; --j) {
     if (j != nLevels) {
       initP2PNonLeaf(j);

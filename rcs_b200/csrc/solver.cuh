@@ -19,10 +19,12 @@ struct SolverParams {
   int leafSize = 64, tol_pow = 8, nLevelsInput = 0, fillin_rank = 0, fillin_tol = 10;
   int realMode = 0;      // electrostatics: real Householder sign in RRQR
   size_t aca_budget = (size_t)24 << 30;  // bytes of ACA workspace per launch
+  bool phaseTiming = false;              // synchronise at phase boundaries for exact phase times
 };
 
 struct SolverStats {
   double t_assemble = 0, t_factor = 0, t_solve = 0;
+  double t_rrqr = 0, t_compress = 0, t_elim_x = 0, t_elim_z = 0, t_nonleaf = 0;
   double flops_factor = 0;  // complex-counted algorithmic flops issued by the factorization
   long nRRQR = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
   long kernels = 0;

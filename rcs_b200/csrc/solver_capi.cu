@@ -1,26 +1,12 @@
 // C ABI of the AIFMM solver (see include/aifmm_b200.h).
+#include <cstdlib>
 #include <memory>
 
+#include "capi_guard.cuh"
 #include "solver.cuh"
 
 using namespace aifmm;
 
-#define API_BEGIN try {
-#define API_END                               \
-  }                                           \
-  catch (const Error& e) {                    \
-    set_last_error(e.what());                 \
-    return e.code;                            \
-  }                                           \
-  catch (const std::bad_alloc&) {             \
-    set_last_error("host allocation failed"); \
-    return AIFMM_ENOMEM;                      \
-  }                                           \
-  catch (const std::exception& e) {           \
-    set_last_error(e.what());                 \
-    return AIFMM_EINVAL;                      \
-  }                                           \
-  return AIFMM_OK;
 
 extern "C" {
 
@@ -37,6 +23,8 @@ int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_sol
   sp.fillin_rank = p->fillin_rank;
   sp.nLevelsInput = p->n_levels;
   sp.realMode = k->geom.efie ? 0 : 1;
+  const char* pt = std::getenv("AIFMM_PHASE_TIMES");
+  sp.phaseTiming = pt && pt[0] == '1';
   std::unique_ptr<aifmm_solver> s(new aifmm_solver);
   s->s.reset(new Solver(k, sp));
   s->s->build();
@@ -104,6 +92,11 @@ int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
   info->flops_factor = S.stats.flops_factor;
   info->mem_gb = S.memoryGB(false);
   info->mem_after_gb = S.memoryGB(true);
+  info->t_rrqr = S.stats.t_rrqr;
+  info->t_compress = S.stats.t_compress;
+  info->t_elim_x = S.stats.t_elim_x;
+  info->t_elim_z = S.stats.t_elim_z;
+  info->t_nonleaf = S.stats.t_nonleaf;
   API_END
 }
 

@@ -99,6 +99,31 @@ class AIFMM:
     def getPhi(self) -> np.ndarray:
         return self._x
 
+    def solve_gmres(self, A: "H2Operator", rhs, tol: float = 1e-6, restart: int = 30,
+                    maxit: int = 200) -> tuple[np.ndarray, dict]:
+        """Flexible GMRES(restart) on the forward operator A, right-preconditioned
+        by this factorization; returns x and the iteration record."""
+        b = np.asarray(rhs, dtype=np.complex128)
+        one = b.ndim == 1
+        B = b.reshape(self.N, -1)
+        nrhs = B.shape[1]
+        flat = np.ascontiguousarray(B.T).ravel()
+        X = np.zeros(self.N * nrhs, dtype=np.complex128)
+        gi = _lib.GmresInfo()
+        _lib.check(_lib.lib().aifmm_solver_solve_gmres(self.h, A.h, flat.view(np.float64), nrhs, X.view(np.float64),
+                                                       float(tol), int(restart), int(maxit), C.byref(gi)))
+        Xm = X.reshape(nrhs, self.N).T
+        rec = {f: getattr(gi, f) for f, _ in gi._fields_}
+        return (Xm[:, 0].copy() if one else Xm.copy()), rec
+
+    def solve_gmres_device(self, A: "H2Operator", rhs_ptr: int, nrhs: int, x_ptr: int, tol: float = 1e-6,
+                           restart: int = 30, maxit: int = 200) -> dict:
+        gi = _lib.GmresInfo()
+        _lib.check(_lib.lib().aifmm_solver_solve_gmres_device(self.h, A.h, C.c_void_p(rhs_ptr), int(nrhs),
+                                                              C.c_void_p(x_ptr), float(tol), int(restart),
+                                                              int(maxit), C.byref(gi)))
+        return {f: getattr(gi, f) for f, _ in gi._fields_}
+
     def info(self) -> dict:
         i = _lib.SolverInfo()
         _lib.check(_lib.lib().aifmm_solver_get_info(self.h, C.byref(i)))
@@ -119,6 +144,50 @@ class AIFMM:
     def rewind(self) -> None:
         """Restore the checkpointed operator so that factorize can run again."""
         _lib.check(_lib.lib().aifmm_solver_rewind(self.h))
+
+
+class H2Operator:
+    """FP64 forward operator y = A x of the kernel in H^2 form: the assembly of
+    AIFMM (octree, ACA skeletons, L2P/P2M, M2L, leaf P2P) at ACA tolerance
+    10^-tol_pow, kept unfactorized.  The residual operator of
+    AIFMM.solve_gmres; the reference has no counterpart."""
+
+    def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 10, n_levels: int = 0):
+        p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(tol_pow), 0, int(n_levels), 0)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().aifmm_operator_create(K.h, C.byref(p), C.byref(h)))
+        self.h = h
+        self.N = K.N
+
+    def close(self):
+        if getattr(self, "h", None):
+            _lib.lib().aifmm_operator_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __matmul__(self, x) -> np.ndarray:
+        b = np.asarray(x, dtype=np.complex128)
+        one = b.ndim == 1
+        B = b.reshape(self.N, -1)
+        nrhs = B.shape[1]
+        flat = np.ascontiguousarray(B.T).ravel()
+        Y = np.zeros(self.N * nrhs, dtype=np.complex128)
+        _lib.check(_lib.lib().aifmm_operator_apply(self.h, flat.view(np.float64), nrhs, Y.view(np.float64)))
+        Ym = Y.reshape(nrhs, self.N).T
+        return Ym[:, 0].copy() if one else Ym.copy()
+
+    def apply_device(self, x_ptr: int, nrhs: int, y_ptr: int) -> None:
+        _lib.check(_lib.lib().aifmm_operator_apply_device(self.h, C.c_void_p(x_ptr), int(nrhs), C.c_void_p(y_ptr)))
+
+    def info(self) -> dict:
+        b, f = C.c_double(), C.c_double()
+        _lib.check(_lib.lib().aifmm_operator_info(self.h, C.byref(b), C.byref(f)))
+        return {"bytes": b.value, "flops_per_column": f.value}
 
 
 def launch_count() -> int:
