@@ -388,8 +388,98 @@ void zgetrf(aifmm_ctx* ctx, zd* A, int n, int lda, int* piv, int* info) {
   }
 }
 
+// Whole solve for a few right-hand sides in one CTA: B staged in shared
+// memory (n x nrhs, ld n), row interchanges, then forward (unit lower) and
+// backward (upper) substitution in 32-row blocks -- a warp per right-hand
+// side solves the diagonal block with lane = row, then all threads update
+// the remaining rows, thread = (row, column).
+constexpr int GS_NT = 256;
+constexpr size_t GS_SMEM_MAX = 200 * 1024;
+
+__global__ void __launch_bounds__(GS_NT) zgetrs_smem_kernel(const zd* __restrict__ LU, int n, int lda,
+                                                            const int* __restrict__ piv, zd* B, int nrhs, int ldb) {
+  extern __shared__ zd xs[];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int t = tid; t < n * nrhs; t += GS_NT) xs[t] = B[(size_t)(t / n) * ldb + (t % n)];
+  __syncthreads();
+  if (tid < nrhs) {
+    zd* x = xs + (size_t)tid * n;
+    for (int k = 0; k < n; ++k) {
+      const int p = piv[k];
+      if (p != k) {
+        const zd t = x[k];
+        x[k] = x[p];
+        x[p] = t;
+      }
+    }
+  }
+  __syncthreads();
+  for (int b0 = 0; b0 < n; b0 += 32) {  // forward, unit lower
+    const int nb = min(32, n - b0);
+    for (int c = warp; c < nrhs; c += GS_NT / 32) {
+      zd* x = xs + (size_t)c * n + b0;
+      zd xi = lane < nb ? x[lane] : zmk(0, 0);
+      for (int l = 0; l < nb; ++l) {
+        zd xl;
+        xl.x = __shfl_sync(0xffffffff, xi.x, l);
+        xl.y = __shfl_sync(0xffffffff, xi.y, l);
+        if (lane > l && lane < nb) xi = zsub(xi, zmul(LU[(size_t)(b0 + l) * lda + b0 + lane], xl));
+      }
+      if (lane < nb) x[lane] = xi;
+    }
+    __syncthreads();
+    const int r0 = b0 + nb, rest = n - r0;
+    for (int t = tid; t < rest * nrhs; t += GS_NT) {
+      const int i = r0 + t % rest, c = t / rest;
+      const zd* xb = xs + (size_t)c * n + b0;
+      zd s = zmk(0, 0);
+      for (int l = 0; l < nb; ++l) s = zadd(s, zmul(LU[(size_t)(b0 + l) * lda + i], xb[l]));
+      xs[(size_t)c * n + i] = zsub(xs[(size_t)c * n + i], s);
+    }
+    __syncthreads();
+  }
+  for (int b0 = ((n - 1) / 32) * 32; b0 >= 0; b0 -= 32) {  // backward, upper
+    const int nb = min(32, n - b0);
+    for (int c = warp; c < nrhs; c += GS_NT / 32) {
+      zd* x = xs + (size_t)c * n + b0;
+      zd xi = lane < nb ? x[lane] : zmk(0, 0);
+      for (int l = nb - 1; l >= 0; --l) {
+        if (lane == l) xi = zdiv(xi, LU[(size_t)(b0 + l) * lda + b0 + l]);
+        zd xl;
+        xl.x = __shfl_sync(0xffffffff, xi.x, l);
+        xl.y = __shfl_sync(0xffffffff, xi.y, l);
+        if (lane < l) xi = zsub(xi, zmul(LU[(size_t)(b0 + l) * lda + b0 + lane], xl));
+      }
+      if (lane < nb) x[lane] = xi;
+    }
+    __syncthreads();
+    for (int t = tid; t < b0 * nrhs; t += GS_NT) {
+      const int i = t % b0, c = t / b0;
+      const zd* xb = xs + (size_t)c * n + b0;
+      zd s = zmk(0, 0);
+      for (int l = 0; l < nb; ++l) s = zadd(s, zmul(LU[(size_t)(b0 + l) * lda + i], xb[l]));
+      xs[(size_t)c * n + i] = zsub(xs[(size_t)c * n + i], s);
+    }
+    __syncthreads();
+  }
+  for (int t = tid; t < n * nrhs; t += GS_NT) B[(size_t)(t / n) * ldb + (t % n)] = xs[t];
+}
+
 void zgetrs(aifmm_ctx* ctx, const zd* LU, int n, int lda, const int* piv, zd* B, int nrhs, int ldb) {
   if (n <= 0 || nrhs <= 0) return;
+  const size_t smem = sizeof(zd) * (size_t)n * nrhs;
+  if (nrhs <= 16 && smem <= GS_SMEM_MAX) {
+    static bool attr[256] = {};  // the attribute is set once per device
+    AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
+    if (!attr[ctx->device]) {
+      AIFMM_CUDA(cudaFuncSetAttribute(zgetrs_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)GS_SMEM_MAX));
+      attr[ctx->device] = true;
+    }
+    zgetrs_smem_kernel<<<1, GS_NT, smem, ctx->stream>>>(LU, n, lda, piv, B, nrhs, ldb);
+    AIFMM_LAUNCHED();
+    return;
+  }
   zlaswp_kernel<<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(B, ldb, nrhs, piv, n);
   AIFMM_LAUNCHED();
   // forward: unit lower

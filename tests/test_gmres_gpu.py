@@ -29,15 +29,21 @@ def _relerr(A, B):
     return float(np.linalg.norm(A - B) / np.linalg.norm(B))
 
 
-@pytest.mark.parametrize("sub,freq,leaf,tol_pow", [
-    (3, 1.0e9, 64, 10),   # 1,920 unknowns, the c1 sphere
-    (3, 4.0e9, 32, 10),   # electrically larger, deeper tree
-    (2, 1.0e9, 16, 10),   # 480 unknowns
+def _far_field_present(A, N):
+    return A.info()["bytes"] < 0.9 * 16.0 * N * N  # some blocks are stored in low-rank form
+
+
+@pytest.mark.parametrize("sub,freq,leaf,levels,tol_pow", [
+    (3, 1.0e9, 64, 0, 10),    # 1,920 unknowns, the c1 sphere, the reference's depth rule
+    (3, 4.0e9, 16, 3, 10),    # electrically larger, three levels
+    (4, 2.0e9, 32, 3, 10),    # 7,680 unknowns
 ])
-def test_operator_matches_dense(sub, freq, leaf, tol_pow):
+def test_operator_matches_dense(sub, freq, leaf, levels, tol_pow):
     K = EFIEMatrix(M.icosphere(sub, 0.15), freq)
     Z = _dense(K)
-    A = H2Operator(K, leaf_size=leaf, tol_pow=tol_pow)
+    A = H2Operator(K, leaf_size=leaf, tol_pow=tol_pow, n_levels=levels)
+    if levels == 3:
+        assert _far_field_present(A, K.N)
     X = _rhs(K.N, 3, 1)
     Y = A @ X
     err = _relerr(Y, Z @ X)
@@ -50,15 +56,18 @@ def test_operator_tolerance_controls_error():
     K = EFIEMatrix(M.icosphere(3, 0.15), 1.0e9)
     Z = _dense(K)
     X = _rhs(K.N, 2, 5)
-    errs = [_relerr(H2Operator(K, leaf_size=32, tol_pow=t) @ X, Z @ X) for t in (4, 7, 10)]
+    ops = [H2Operator(K, leaf_size=16, tol_pow=t, n_levels=3) for t in (4, 7, 10)]
+    assert all(_far_field_present(A, K.N) for A in ops)
+    errs = [_relerr(A @ X, Z @ X) for A in ops]
     assert errs[0] > errs[1] > errs[2], errs
+    assert errs[2] < 1e-7, errs
 
 
 def test_operator_column_chunks():
     """More columns than one skinny pass takes (16) go through in chunks."""
     K = EFIEMatrix(M.icosphere(2, 0.15), 1.0e9)
     Z = _dense(K)
-    A = H2Operator(K, leaf_size=16, tol_pow=10)
+    A = H2Operator(K, leaf_size=8, tol_pow=10, n_levels=3)
     X = _rhs(K.N, 19, 2)
     assert _relerr(A @ X, Z @ X) < 1e-7
 
@@ -66,7 +75,8 @@ def test_operator_column_chunks():
 def test_operator_electrostatics():
     K = ElectrostaticsMatrix(M.icosphere(3, 1.0))
     Z = _dense(K)
-    A = H2Operator(K, leaf_size=32, tol_pow=10)
+    A = H2Operator(K, leaf_size=16, tol_pow=10, n_levels=3)
+    assert _far_field_present(A, K.N)
     X = _rhs(K.N, 2, 3)
     assert _relerr(A @ X, Z @ X) < 1e-7
 
@@ -77,9 +87,9 @@ def test_gmres_reaches_dense_residual(tol):
     ||Z x - b|| / ||b|| with the dense matrix meets the target."""
     K = EFIEMatrix(M.icosphere(3, 0.15), 1.0e9)
     Z = _dense(K)
-    S = AIFMM(K, leaf_size=64, tol_pow=4, fillin_tol=6)
+    S = AIFMM(K, leaf_size=16, tol_pow=4, fillin_tol=6, n_levels=3)
     S.factorize()
-    A = H2Operator(K, leaf_size=64, tol_pow=11)
+    A = H2Operator(K, leaf_size=16, tol_pow=11, n_levels=3)
     B = np.stack([K.planeWaveRhs((0, 0, -1), (1, 0, 0)), K.planeWaveRhs((1, 0, 0), (0, 1, 0)),
                   _rhs(K.N, 1, 4)[:, 0]], axis=1)
     direct_res = np.linalg.norm(Z @ S.solve(B) - B) / np.linalg.norm(B)
