@@ -31,19 +31,27 @@ sys.path.insert(0, ROOT)
 METRIC = "factor+solve s at rel. residual 1e-6: mixed/batched/learned vs plain FP64 GPU"
 
 # Workloads; synthetic icosphere meshes, seeded plane waves.
+# tol_pow / fillin_tol: the factorization's ACA and RRQR tolerances; op_tol:
+# ACA tolerance of the FP64 H^2 forward operator that GMRES iterates on; gmres:
+# target relative residual (None = direct solve only, the reference's path).
 CONFIGS = {
-    "c1": dict(sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0,
-               desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10"),
-    "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=7, fillin_tol=9, nrhs=8, levels=0,
-               desc="EFIE PEC sphere R=0.15 m f=4 GHz, 81,920 tri, N=122,880, leaf 128, ACA 1e-7, RRQR 1e-9, "
-                    "8 plane waves"),
-    "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=7, fillin_tol=9, nrhs=8, levels=0,
-                desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-7, RRQR 1e-9, "
-                     "8 plane waves (c3 shape at 1/4 size)"),
+    "c1": dict(sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0, op_tol=None,
+               gmres=None,
+               desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10, "
+                    "direct solve"),
+    "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
+               gmres=1e-6,
+               desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
+                    "RRQR 1e-7, 8 seeded plane waves, FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
+    "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
+                gmres=1e-6,
+                desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
+                     "8 plane waves, FGMRES(30) to 1e-6 (c3 shape at 1/4 size)"),
 }
-# CPU sample for the reference arm and cpu_baseline: same tree depth as c3
-# (nLevels = 3, N / leaf = 960) at 1/16 of the unknowns.
-CPU_SAMPLE = dict(sub=4, radius=0.15, freq=1.0e9, leaf=8, tol_pow=7, fillin_tol=9, nrhs=1, levels=0)
+# CPU sample for the reference arm and cpu_baseline: the c3 sphere and
+# frequency on the 1,280-triangle mesh (N=1,920) with c3's tree depth (3
+# levels) and tolerances; about 25 s of oracle factor+solve on 8 cores.
+CPU_SAMPLE = dict(sub=3, radius=0.15, freq=4.0e9, leaf=8, tol_pow=5, fillin_tol=7, nrhs=1, levels=3)
 
 
 def plane_waves(n: int, seed: int = 4):
@@ -130,9 +138,12 @@ def barrier(world: int):
 
 
 def build_workload(cfg, device: int):
+    """Mesh, kernel, right-hand sides, the assembled (checkpointed) solver and,
+    when the config refines, the FP64 forward operator.  Not timed as a step:
+    the reference times assembly separately from factor+solve."""
     from rcs_b200 import mesh as M
     from rcs_b200.kernel import Context, EFIEMatrix
-    from rcs_b200.solver import AIFMM
+    from rcs_b200.solver import AIFMM, H2Operator
     ctx = Context(device)
     m = M.icosphere(cfg["sub"], cfg["radius"])
     K = EFIEMatrix(m, cfg["freq"], ctx=ctx)
@@ -142,7 +153,12 @@ def build_workload(cfg, device: int):
     S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"])
     t_asm = time.perf_counter() - t0
     S.checkpoint()
-    return ctx, m, K, S, B, t_asm
+    A, t_op = None, 0.0
+    if cfg.get("op_tol") is not None:
+        t0 = time.perf_counter()
+        A = H2Operator(K, leaf_size=cfg["leaf"], tol_pow=cfg["op_tol"], n_levels=cfg["levels"])
+        t_op = time.perf_counter() - t0
+    return ctx, m, K, S, A, B, t_asm, t_op
 
 
 def sampled_residual(K, X: np.ndarray, B: np.ndarray, nrows: int = 2048, seed: int = 1) -> float:
@@ -178,9 +194,8 @@ def zgemm_peak_tflops() -> float:
 
 
 def cpu_sample_seconds(threads: int):
-    """Oracle (the reference's CPU algorithm restated) factor+solve on the CPU
-    sample, and the same sample's algorithmic factorization flops (counted by
-    the GPU run of the identical algorithm)."""
+    """Oracle (the reference's CPU algorithm restated) factor + direct solve on
+    the CPU sample; returns seconds and the sample's unknown count."""
     import oracle
     from rcs_b200 import mesh as M
     oracle.set_threads(threads)
@@ -192,7 +207,28 @@ def cpu_sample_seconds(threads: int):
     t0 = time.perf_counter()
     S.factorize()
     S.solve(b)
-    return time.perf_counter() - t0, m
+    return time.perf_counter() - t0
+
+
+def factor_flops(c, ctx) -> float:
+    """Algorithmic factorization flops of a config, counted by the GPU run of
+    the same algorithm (the oracle cannot run the full workload in minutes)."""
+    from rcs_b200 import mesh as M
+    from rcs_b200.kernel import EFIEMatrix
+    from rcs_b200.solver import AIFMM
+    K = EFIEMatrix(M.icosphere(c["sub"], c["radius"]), c["freq"], ctx=ctx)
+    S = AIFMM(K, leaf_size=c["leaf"], tol_pow=c["tol_pow"], fillin_tol=c["fillin_tol"], n_levels=c["levels"])
+    S.factorize()
+    f = S.info()["flops_factor"]
+    S.close()
+    K.close()
+    return f
+
+
+def sample_text(t_sample: float, scale: float) -> str:
+    return (f"oracle (C++ restatement of the reference, OpenMP) factor + direct solve of the c3 sphere at f=4 GHz "
+            f"on icosphere {CPU_SAMPLE['sub']} (N=1,920, leaf {CPU_SAMPLE['leaf']}, 3 levels, ACA 1e-5, RRQR 1e-7) "
+            f"= {t_sample:.2f} s, scaled to the workload by factorization flops x{scale:.1f}")
 
 
 def run_reference(args, rank, world):
@@ -203,33 +239,24 @@ def run_reference(args, rank, world):
         return
     cfg = CONFIGS[args.config]
     threads = os.cpu_count() or 1
-    # flops of the full workload and of the sample, from GPU runs of the same algorithm
-    from rcs_b200 import mesh as M
-    from rcs_b200.kernel import Context, EFIEMatrix
-    from rcs_b200.solver import AIFMM
+    from rcs_b200.kernel import Context
     ctx = Context(0)
-    flops = {}
-    for name, c in (("full", cfg), ("sample", CPU_SAMPLE)):
-        K = EFIEMatrix(M.icosphere(c["sub"], c["radius"]), c["freq"], ctx=ctx)
-        S = AIFMM(K, leaf_size=c["leaf"], tol_pow=c["tol_pow"], fillin_tol=c["fillin_tol"], n_levels=c["levels"])
-        S.factorize()
-        flops[name] = S.info()["flops_factor"]
-        S.close()
-        K.close()
+    scale = factor_flops(cfg, ctx) / factor_flops(CPU_SAMPLE, ctx)
     times = []
-    for _ in range(args.warmup if args.warmup < 1 else 1):
+    for _ in range(min(args.warmup, 1)):
         cpu_sample_seconds(threads)
     for _ in range(args.steps):
-        t, _ = cpu_sample_seconds(threads)
-        times.append(t * flops["full"] / flops["sample"])
-    v = float(np.mean(times))
+        times.append(cpu_sample_seconds(threads))
+    t_s = float(np.mean(times))
+    v = t_s * scale
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": cfg["desc"], "parallelism": "replicas"},
+            "config": {"workload": cfg["desc"], "parallelism": "replicas" if world > 1 else "single process",
+                       "reference_path": "factor + direct solve at the config's ACA/RRQR tolerances (the reference "
+                                         "has no refinement)"},
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
-                             "sample": f"oracle factor+solve of icosphere {CPU_SAMPLE['sub']} (N=7,680, leaf 8, "
-                                       f"same depth) scaled by factorization flops x{flops['full'] / flops['sample']:.1f}"},
+                             "sample": sample_text(t_s, scale)},
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -245,10 +272,9 @@ def main():
     args = ap.parse_args()
     rank, world, local = dist_env()
     if world > 1:
-        import torch
         import torch.distributed as dist
         from datetime import timedelta
-        dist.init_process_group("gloo", timeout=timedelta(seconds=600))
+        dist.init_process_group("gloo", timeout=timedelta(seconds=900))
     if args.impl == "reference":
         run_reference(args, rank, world)
         if world > 1:
@@ -259,21 +285,27 @@ def main():
     torch.cuda.set_device(local)
     from rcs_b200.solver import launch_count, profile_gemm, profile_gemm_read
     cfg = CONFIGS[args.config]
-    ctx, m, K, S, B, t_asm = build_workload(cfg, local)
+    ctx, m, K, S, A, B, t_asm, t_op = build_workload(cfg, local)
     N, nrhs = K.N, B.shape[1]
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
     Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(f"cuda:{local}")  # nrhs x N == column-major N x nrhs
     Xd = torch.empty_like(Bd)
+    recs = []
 
     def step():
         S.rewind()
         S.factorize()
-        S.solve_device(Bd.data_ptr(), nrhs, Xd.data_ptr())
+        if A is None:
+            S.solve_device(Bd.data_ptr(), nrhs, Xd.data_ptr())
+        else:
+            recs.append(S.solve_gmres_device(A, Bd.data_ptr(), nrhs, Xd.data_ptr(), tol=cfg["gmres"], restart=30,
+                                             maxit=300))
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
     barrier(world)
+    recs.clear()
     l0 = launch_count()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
@@ -289,22 +321,33 @@ def main():
     X = Xd.cpu().numpy().T
     res = sampled_residual(K, X, B)
     info = S.info()
+    gm = None
+    if recs:
+        gm = {"iterations_per_step": [r["iterations"] for r in recs], "relres_operator": max(r["relres"] for r in recs),
+              "precond_s_per_step": float(np.mean([r["t_precond"] for r in recs])),
+              "matvec_s_per_step": float(np.mean([r["t_matvec"] for r in recs]))}
 
     # e2e: the public host API, pinned host buffers, H2D/D2H inside the step
     Bh = torch.from_numpy(np.ascontiguousarray(B.T)).pin_memory()
     Xh = torch.empty_like(Bh).pin_memory()
     from rcs_b200 import _lib
     import ctypes as C
+    hb = np.ctypeslib.as_array(C.cast(Bh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))
+    hx = np.ctypeslib.as_array(C.cast(Xh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     for _ in range(args.steps):
         S.rewind()
-        S.factorize()
-        _lib.check(_lib.lib().aifmm_solver_solve(S.h, np.ctypeslib.as_array(
-            C.cast(Bh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,)), nrhs,
-            np.ctypeslib.as_array(C.cast(Xh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))))
+        _lib.check(_lib.lib().aifmm_solver_factorize(S.h))
+        if A is None:
+            _lib.check(_lib.lib().aifmm_solver_solve(S.h, hb, nrhs, hx))
+        else:
+            gi = _lib.GmresInfo()
+            _lib.check(_lib.lib().aifmm_solver_solve_gmres(S.h, A.h, hb, nrhs, hx, float(cfg["gmres"]), 30, 300,
+                                                           C.byref(gi)))
     t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    res_e2e = sampled_residual(K, Xh.numpy().T, B, nrows=512)
 
     # roofline of the dominant kernel (grouped complex GEMM) over one more step
     profile_gemm(True)
@@ -318,29 +361,25 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t_s, _ = cpu_sample_seconds(threads)
-        # scale by the factorization flops of the workload vs the sample
-        from rcs_b200 import mesh as M
-        from rcs_b200.kernel import EFIEMatrix
-        from rcs_b200.solver import AIFMM
-        Ks = EFIEMatrix(M.icosphere(CPU_SAMPLE["sub"], CPU_SAMPLE["radius"]), CPU_SAMPLE["freq"], ctx=ctx)
-        Ss = AIFMM(Ks, leaf_size=CPU_SAMPLE["leaf"], tol_pow=CPU_SAMPLE["tol_pow"],
-                   fillin_tol=CPU_SAMPLE["fillin_tol"], n_levels=CPU_SAMPLE["levels"])
-        Ss.factorize()
-        scale = info["flops_factor"] / max(Ss.info()["flops_factor"], 1.0)
-        cpu = {"value": t_s * scale, "unit": "s", "cores": threads, "kind": "port",
-               "sample": f"oracle factor+solve of icosphere {CPU_SAMPLE['sub']} (N=7,680, leaf 8, same tree depth) "
-                         f"= {t_s:.2f} s, scaled by factorization flops x{scale:.1f}"}
+        t_s = cpu_sample_seconds(threads)
+        scale = info["flops_factor"] / max(factor_flops(CPU_SAMPLE, ctx), 1.0)
+        cpu = {"value": t_s * scale, "unit": "s", "cores": threads, "kind": "port", "sample": sample_text(t_s, scale)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs, "path": "plain complex128 (reference control flow)",
+            "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs,
+                       "path": "plain complex128 factorization (reference control flow) + FP64 FGMRES"
+                       if A is not None else "plain complex128 (reference control flow), direct solve",
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"},
-            "residual": res, "residual_rows_sampled": min(2048, N),
-            "assemble_s": t_asm, "factor_flops": info["flops_factor"],
+            "residual": res, "residual_e2e": res_e2e, "residual_rows_sampled": min(2048, N),
+            "residual_reference": "||Z x - b|| / ||b|| over seeded rows with exact FP64 matrix entries",
+            "gmres": gm, "assemble_s": t_asm, "operator_build_s": t_op,
+            "operator_gb": (A.info()["bytes"] / 1e9) if A is not None else None,
+            "factor_flops": info["flops_factor"],
+            "phases_s": {k: info[k] for k in ("t_rrqr", "t_compress", "t_elim_x", "t_elim_z", "t_nonleaf")},
             "tree": {"levels": info["n_levels"], "avg_leaf": info["avg_leaf_size"], "avg_rank": info["avg_multipoles"],
                      "max_rank": info["max_rank"], "rrqr": info["n_rrqr"]},
             "gpu_launches": int(launches),

@@ -142,6 +142,12 @@ typedef struct {
   int fillin_rank; /* accepted for compatibility; the reference's active path ignores it */
   int n_levels;    /* 0 = the reference's rule max(2, floor(log8(N / leaf))) */
   int precision;   /* 0 = plain complex128 (the reference's arithmetic) */
+  int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
+                    * Householder pass, as the reference does; 0 (default) skips
+                    * that pass when the old basis is one this solver produced with
+                    * orthonormal columns: its partition 1 then keeps every column,
+                    * so only the fill-in's component outside the old span is
+                    * factorized (same ranks and spans, different rounding) */
 } aifmm_solver_params;
 
 typedef struct {

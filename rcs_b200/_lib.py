@@ -70,7 +70,7 @@ SIGNATURES = {
 
 class SolverParams(C.Structure):
     _fields_ = [("leaf_size", C.c_int), ("tol_pow", C.c_int), ("fillin_tol", C.c_int), ("fillin_rank", C.c_int),
-                ("n_levels", C.c_int), ("precision", C.c_int)]
+                ("n_levels", C.c_int), ("precision", C.c_int), ("exact_rrqr", C.c_int)]
 
 
 class SolverInfo(C.Structure):

@@ -97,6 +97,7 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
   P.maxPivot = (double*)((char*)out.p + 8);
   P.istate = (int*)((char*)out.p + 16);
   P.dstate = (double*)((char*)out.p + 32);
+  P.p2cap = -1;
   launch_rrqr_split(ctx, {P});
   struct {
     int r, pad;

@@ -595,8 +595,9 @@ __global__ void __launch_bounds__(QR_NT) rrqr_p2_kernel(const RRQRProblem* __res
   const int partition = P.partition;
   for (int q = rank_p1 + tid; q < partition; q += QR_NT) P.nsq[q] = 0.0;
   __syncthreads();
-  const int steps = min(m, n) - (partition - rank_p1);
+  int steps = min(m, n) - (partition - rank_p1);
   const int first = rank_p1;
+  if (P.p2cap >= 0) steps = min(steps, first + P.p2cap);
   int rank_p2 = min(steps - first, m);
   for (int j = first; j < steps; ++j)
     if (!rrqr_step_dev(P, j, n, n, false, first, nref, mp1, maxPivot, shv, shi, s_alpha)) {

@@ -43,6 +43,7 @@ struct RRQRProblem {
   double* maxPivot;  // out
   int* istate;       // split pipeline only: 4 ints of scratch
   double* dstate;    // split pipeline only: 2 doubles of scratch
+  int p2cap;         // split pipeline only: at most this many partition-2 steps (-1: no cap)
 };
 
 // Single-kernel RRQR (one CTA per problem).

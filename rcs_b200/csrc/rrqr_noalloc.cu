@@ -98,6 +98,7 @@ extern "C" int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partit
     P.maxPivot = max_pivot_device;
     P.istate = nullptr;  // the single-kernel form keeps its state in registers
     P.dstate = nullptr;
+    P.p2cap = -1;
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     RRQRProblem* desc = reinterpret_cast<RRQRProblem*>(b);
     const int grid = (int)std::min<size_t>(((size_t)m * n + 255) / 256, 148 * 4);

@@ -514,11 +514,11 @@ bool Solver::wellSeparated(int j, int k, int l) const {  // T:4044-4055
   return true;
 }
 
-DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot) {
-  PhaseTimer pt(*this, stats.t_rrqr);
-  const int m = A.r, n = A.c;
+// Partitioned column-pivoted QR of the working copy R (destroyed); returns
+// Q_trunc.  p2cap bounds the partition-2 steps (-1: none).
+DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot) {
+  const int m = R.r, n = R.c;
   const int hs = std::min(m, n) + 1;
-  DMat R = ops.copy(A);
   DevBuf H(ctx, sizeof(zd) * (size_t)m * hs + 16), Q(ctx, sizeof(zd) * (size_t)m * hs + 16);
   DevBuf nsq(ctx, sizeof(double) * n + 8), perm(ctx, sizeof(int) * n + 8), out(ctx, 64);
   RRQRProblem P;
@@ -539,9 +539,9 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
   P.maxPivot = (double*)((char*)out.p + 8);
   P.istate = (int*)((char*)out.p + 16);
   P.dstate = (double*)((char*)out.p + 32);
+  P.p2cap = p2cap;
   launch_rrqr_split(ctx, {P});
   stats.kernels += 4;
-  stats.nRRQR++;
   struct {
     int rank, pad;
     double mp;
@@ -552,6 +552,48 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
   maxPivot = h.mp;
   DMat Qt = ops.alloc(m, h.rank);
   if (Qt.size()) AIFMM_CUDA(cudaMemcpyAsync(Qt.p, Q.p, sizeof(zd) * Qt.size(), cudaMemcpyDeviceToDevice, ctx->stream));
+  return Qt;
+}
+
+// RRQR of A = [old basis (partition columns) | fill-in] (rrqr.cpp:98-182).
+// When the old basis has orthonormal columns (orthoPanel), partition 1 of the
+// reference keeps every one of them -- each pivot is the unit norm of a
+// column orthogonal to the ones before, never below tol1 <= 1 -- so its
+// Householder pass only re-expresses the same span.  The shortcut keeps the
+// old basis as it is, projects the fill-in onto its orthogonal complement
+// (classical Gram-Schmidt, twice) and runs partition 2 on the projection with
+// the reference's step bound min(m - partition, fill-in columns); ranks,
+// pivots and spans are those of the full pass, the basis of the old span is
+// the identity instead of a Householder rotation of it, and maxPivot of an
+// empty partition 2 is the unit norm of the first old column.
+DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel) {
+  PhaseTimer pt(*this, stats.t_rrqr);
+  const int m = A.r, n = A.c;
+  stats.nRRQR++;
+  if (!(orthoPanel && prm.orthoShortcut && partition > 0 && partition <= m))
+    return rrqrRun(ops.copy(A), partition, inputPivot, fillRank, -1, maxPivot);
+  stats.nRRQRShort++;
+  const int r = partition, nf = n - partition;
+  DMat Q1;  // view of the old basis
+  Q1.buf = A.buf;
+  Q1.p = A.p;
+  Q1.r = m;
+  Q1.c = r;
+  if (nf == 0 || m == r) {
+    maxPivot = 1.0;
+    return ops.copy(Q1);
+  }
+  DMat F = ops.block(A, 0, r, m, nf);
+  for (int pass = 0; pass < 2; ++pass) {
+    const DMat C = ops.mul(Q1, OP_C, F, OP_N);
+    GemmBatch g;
+    g.add(F, Q1, OP_N, C, OP_N, MONE, ONE);
+    g.flush(ctx);
+  }
+  const DMat Q2 = rrqrRun(F, 0, inputPivot, fillRank, m - r, maxPivot);
+  DMat Qt = ops.alloc(m, r + Q2.c);
+  zcopy_grouped(ctx, {{Q1.p, Qt.p, m, r, Q1.ld(), Qt.ld(), 0, ONE},
+                      {Q2.p, Qt.p + (size_t)r * Qt.ld(), m, Q2.c, Q2.ld(), Qt.ld(), 0, ONE}});
   return Qt;
 }
 
@@ -608,6 +650,7 @@ void Solver::updateParentL2P(int j, int k, const DMat& nL2P) {  // T:3290-3314
   }
   U[c_k] = ops.mul(ops.mul(nL2P, OP_C, tree[j][k].L2P, OP_N), OP_N, U[c_k], OP_N);
   PL = ops.vcat(U);
+  tree[j - 1][kP].l2pOrtho = false;
 }
 
 void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt) {  // T:3316-3340
@@ -621,16 +664,18 @@ void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt) {  // T:3316-3340
   }
   V[c_b] = ops.mul(ops.mul(V[c_b], OP_N, tree[j][b].P2M, OP_N), OP_N, nP2Mt, OP_N);
   PM = ops.hcatv(V);
+  tree[j - 1][bP].p2mOrtho = false;
 }
 
 void Solver::compressP2PRRQR(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& P2Pt,
                              DMat& nL2P, DMat& nP2Mt, DMat& newM2L) {  // T:1573-1656
   double mp1, mp2;
-  nL2P = rrqr(ops.hcat(oldL2P, P2Pt), oldL2P.c, tree[j][k].maxPivot_L2P, fillin_rankVec[j], mp1);
+  nL2P = rrqr(ops.hcat(oldL2P, P2Pt), oldL2P.c, tree[j][k].maxPivot_L2P, fillin_rankVec[j], mp1, tree[j][k].l2pOrtho);
   tree[j][k].maxPivot_L2P = std::max(tree[j][k].maxPivot_L2P, mp1);
   const DMat Rk = ops.mul(nL2P, OP_C, oldL2P, OP_N);
   const DMat Rkp = ops.mul(nL2P, OP_C, P2Pt, OP_N);
-  nP2Mt = rrqr(ops.hcat(ops.adj(oldP2M), ops.adj(Rkp)), oldP2M.r, tree[j][b].maxPivot_P2M, fillin_rankVec[j], mp2);
+  nP2Mt = rrqr(ops.hcat(ops.adj(oldP2M), ops.adj(Rkp)), oldP2M.r, tree[j][b].maxPivot_P2M, fillin_rankVec[j], mp2,
+               tree[j][b].p2mOrtho);
   tree[j][b].maxPivot_P2M = std::max(tree[j][b].maxPivot_P2M, mp2);
   const DMat Rn = ops.mul(nP2Mt, OP_C, oldP2M, OP_C);
   const DMat Rnp = ops.mul(nP2Mt, OP_C, Rkp, OP_C);
@@ -681,6 +726,7 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   }
   tree[j][k].L2P = kL;
   tree[j][b].P2M = ops.adj(bM);
+  tree[j][k].l2pOrtho = tree[j][b].p2mOrtho = true;
   tree[j][k].NumLocals = tree[j][k].L2P.c;
   tree[j][b].NumMultipoles = tree[j][b].P2M.r;
   tree[j][b].M2L[k] = ops.block(M2L_b_k, 0, 0, bL.c, kM.c);
@@ -692,6 +738,7 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   }
   tree[j][b].L2P = bL;
   tree[j][k].P2M = ops.adj(kM);
+  tree[j][b].l2pOrtho = tree[j][k].p2mOrtho = true;
   tree[j][b].NumLocals = tree[j][b].L2P.c;
   tree[j][k].NumMultipoles = tree[j][k].P2M.r;
 }
@@ -703,7 +750,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   DBox& Bk = tree[j][k];
   // compress_M2P_myRRQR(j, k, b)
   double mp;
-  DMat nL2P_k = rrqr(ops.hcat(Bk.L2P, Bk.M2P[b]), Bk.L2P.c, Bk.maxPivot_L2P, fillin_rankVec[j], mp);
+  DMat nL2P_k = rrqr(ops.hcat(Bk.L2P, Bk.M2P[b]), Bk.L2P.c, Bk.maxPivot_L2P, fillin_rankVec[j], mp, Bk.l2pOrtho);
   Bk.maxPivot_L2P = std::max(Bk.maxPivot_L2P, mp);
   DMat M2L_k_b;
   {
@@ -715,7 +762,8 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   }
   // compress_P2L_myRRQR(j, b, k): A_row = [P2M_k^H | P2L[b][k]^H]
   DBox& Bb = tree[j][b];
-  DMat nP2Mt_k = rrqr(ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k])), Bk.P2M.r, Bk.maxPivot_P2M, fillin_rankVec[j], mp);
+  DMat nP2Mt_k =
+      rrqr(ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k])), Bk.P2M.r, Bk.maxPivot_P2M, fillin_rankVec[j], mp, Bk.p2mOrtho);
   Bk.maxPivot_P2M = std::max(Bk.maxPivot_P2M, mp);
   DMat M2L_b_k;
   {
@@ -732,11 +780,13 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   updateOtherM2LsAtK(j, k, b, kL);
   if (j > startLevel) updateParentL2P(j, k, kL);
   Bk.L2P = kL;
+  Bk.l2pOrtho = true;
   Bk.NumLocals = Bk.L2P.c;
   Bb.M2L[k] = ops.block(M2L_b_k, 0, 0, M2L_b_k.r, kM.c);
   updateOtherM2LsAtB(j, b, k, kM);
   if (j > startLevel) updateParentP2M(j, k, kM);
   Bk.P2M = ops.adj(kM);
+  Bk.p2mOrtho = true;
   Bk.NumMultipoles = Bk.P2M.r;
 }
 
@@ -977,7 +1027,7 @@ void Solver::eliminateZ(int j, int k) {
 void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   const double t0 = wall();
   AIFMM_CUDA(cudaSetDevice(ctx->device));
-  stats.nRRQR = stats.nCompressP2P = stats.nCompressP2L = 0;
+  stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
   stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
   for (int j = nLevels; j >= startLevel; --j) {

@@ -20,13 +20,14 @@ struct SolverParams {
   int realMode = 0;      // electrostatics: real Householder sign in RRQR
   size_t aca_budget = (size_t)24 << 30;  // bytes of ACA workspace per launch
   bool phaseTiming = false;              // synchronise at phase boundaries for exact phase times
+  bool orthoShortcut = true;             // skip partition 1 of RRQR for orthonormal old bases
 };
 
 struct SolverStats {
   double t_assemble = 0, t_factor = 0, t_solve = 0;
   double t_rrqr = 0, t_compress = 0, t_elim_x = 0, t_elim_z = 0, t_nonleaf = 0;
   double flops_factor = 0;  // complex-counted algorithmic flops issued by the factorization
-  long nRRQR = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
+  long nRRQR = 0, nRRQRShort = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
   long kernels = 0;
 };
 
@@ -43,6 +44,9 @@ struct DBox {
   std::vector<int> chargeLocations, in_charge, in_check, out_charge, out_check;
   DMat Ac, Ar;
   DLU luP2P, luL2M;  // stored factors of P2P[k] and L2M_f (the reference recomputes them in the sweeps)
+  // L2P has orthonormal columns / P2M orthonormal rows because a recompression
+  // of this box produced them (not the ACA interpolation, not a parent update)
+  bool l2pOrtho = false, p2mOrtho = false;
   bool hasLuP2P = false, hasLuL2M = false;
 };
 
@@ -103,7 +107,8 @@ class Solver {
   void updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt);
   void updateParentL2P(int j, int k, const DMat& nL2P);
   void updateParentP2M(int j, int b, const DMat& nP2Mt);
-  DMat rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot);
+  DMat rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel);
+  DMat rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot);
   void assignLeafRhs(const DMat& rhs);
   void rhsEliminateX(int j, int k);
   void rhsEliminateZ(int j, int k);

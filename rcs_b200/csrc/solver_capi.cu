@@ -22,6 +22,7 @@ int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_sol
   sp.fillin_tol = p->fillin_tol;
   sp.fillin_rank = p->fillin_rank;
   sp.nLevelsInput = p->n_levels;
+  sp.orthoShortcut = p->exact_rrqr == 0;
   sp.realMode = k->geom.efie ? 0 : 1;
   const char* pt = std::getenv("AIFMM_PHASE_TIMES");
   sp.phaseTiming = pt && pt[0] == '1';

@@ -46,9 +46,9 @@ class _TreeView:
 
 class AIFMM:
     def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 8, fillin_tol: int = 10,
-                 fillin_rank: int = 0, n_levels: int = 0, precision: int = 0):
+                 fillin_rank: int = 0, n_levels: int = 0, precision: int = 0, exact_rrqr: bool = False):
         p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(fillin_tol), int(fillin_rank), int(n_levels),
-                              int(precision))
+                              int(precision), int(bool(exact_rrqr)))
         h = C.c_void_p()
         _lib.check(_lib.lib().aifmm_solver_create(K.h, C.byref(p), C.byref(h)))
         self.h = h
@@ -153,7 +153,7 @@ class H2Operator:
     AIFMM.solve_gmres; the reference has no counterpart."""
 
     def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 10, n_levels: int = 0):
-        p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(tol_pow), 0, int(n_levels), 0)
+        p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(tol_pow), 0, int(n_levels), 0, 0)
         h = C.c_void_p()
         _lib.check(_lib.lib().aifmm_operator_create(K.h, C.byref(p), C.byref(h)))
         self.h = h

@@ -29,10 +29,6 @@ def _relerr(A, B):
     return float(np.linalg.norm(A - B) / np.linalg.norm(B))
 
 
-def _far_field_present(A, N):
-    return A.info()["bytes"] < 0.9 * 16.0 * N * N  # some blocks are stored in low-rank form
-
-
 @pytest.mark.parametrize("sub,freq,leaf,levels,tol_pow", [
     (3, 1.0e9, 64, 0, 10),    # 1,920 unknowns, the c1 sphere, the reference's depth rule
     (3, 4.0e9, 16, 3, 10),    # electrically larger, three levels
@@ -42,8 +38,6 @@ def test_operator_matches_dense(sub, freq, leaf, levels, tol_pow):
     K = EFIEMatrix(M.icosphere(sub, 0.15), freq)
     Z = _dense(K)
     A = H2Operator(K, leaf_size=leaf, tol_pow=tol_pow, n_levels=levels)
-    if levels == 3:
-        assert _far_field_present(A, K.N)
     X = _rhs(K.N, 3, 1)
     Y = A @ X
     err = _relerr(Y, Z @ X)
@@ -53,11 +47,12 @@ def test_operator_matches_dense(sub, freq, leaf, levels, tol_pow):
 
 
 def test_operator_tolerance_controls_error():
+    """The error falls with the ACA tolerance: the far field is in low-rank
+    form (an all-dense operator would be exact at every tolerance)."""
     K = EFIEMatrix(M.icosphere(3, 0.15), 1.0e9)
     Z = _dense(K)
     X = _rhs(K.N, 2, 5)
     ops = [H2Operator(K, leaf_size=16, tol_pow=t, n_levels=3) for t in (4, 7, 10)]
-    assert all(_far_field_present(A, K.N) for A in ops)
     errs = [_relerr(A @ X, Z @ X) for A in ops]
     assert errs[0] > errs[1] > errs[2], errs
     assert errs[2] < 1e-7, errs
@@ -75,10 +70,10 @@ def test_operator_column_chunks():
 def test_operator_electrostatics():
     K = ElectrostaticsMatrix(M.icosphere(3, 1.0))
     Z = _dense(K)
-    A = H2Operator(K, leaf_size=16, tol_pow=10, n_levels=3)
-    assert _far_field_present(A, K.N)
     X = _rhs(K.N, 2, 3)
-    assert _relerr(A @ X, Z @ X) < 1e-7
+    loose = _relerr(H2Operator(K, leaf_size=16, tol_pow=4, n_levels=3) @ X, Z @ X)
+    tight = _relerr(H2Operator(K, leaf_size=16, tol_pow=10, n_levels=3) @ X, Z @ X)
+    assert tight < 1e-7 and loose > 10 * tight, (loose, tight)
 
 
 @pytest.mark.parametrize("tol", [1e-6, 1e-8])

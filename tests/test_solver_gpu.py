@@ -35,16 +35,20 @@ def test_fixture78_matches_oracle_solution():
     assert np.linalg.norm(A @ x - g["rhs"]) / np.linalg.norm(g["rhs"]) < 1e-10
 
 
+@pytest.mark.parametrize("exact", [True, False])
 @pytest.mark.parametrize("sub,freq,leaf,tol,ftol,nl", [
     (3, 1.0e9, 64, 8, 10, 0),   # config 1 with the reference's depth rule (2 levels)
     (3, 1.0e9, 16, 6, 8, 3),    # three levels: RRQR recompression and a non-leaf level
+    (3, 4.0e9, 8, 5, 7, 3),     # loose tolerances, many recompressions of orthonormal bases
 ])
-def test_sphere_matches_oracle(sub, freq, leaf, tol, ftol, nl):
+def test_sphere_matches_oracle(sub, freq, leaf, tol, ftol, nl, exact):
+    """exact=True runs every RRQR through the reference's full partition-1
+    pass; exact=False keeps orthonormal old bases (same ranks and spans)."""
     m = M.icosphere(sub, 0.15)
     K = EFIEMatrix(m, freq)
     O = oracle.EFIE(m, freq)
     b = K.planeWaveRhs((0, 0, -1), (1, 0, 0))
-    S = AIFMM(K, leaf_size=leaf, tol_pow=tol, fillin_tol=ftol, n_levels=nl)
+    S = AIFMM(K, leaf_size=leaf, tol_pow=tol, fillin_tol=ftol, n_levels=nl, exact_rrqr=exact)
     S.factorize()
     x = S.solve(b)
     SO = oracle.AIFMM(O, leaf_size=leaf, tol_pow=tol, fillin_tol=ftol, n_levels=nl)
@@ -71,14 +75,15 @@ def test_multiple_rhs_equal_single_solves():
         assert rel(X[:, c], S.solve(B[:, c])) < 1e-13
 
 
-def test_electrostatics_capacitance():
+@pytest.mark.parametrize("exact,nl", [(True, 0), (False, 0), (False, 3)])
+def test_electrostatics_capacitance(exact, nl):
     m = M.icosphere(3, 1.0)
     K = ElectrostaticsMatrix(m)
     O = oracle.Electrostatics(m)
-    S = AIFMM(K, leaf_size=16, tol_pow=8, fillin_tol=10)
+    S = AIFMM(K, leaf_size=16, tol_pow=8, fillin_tol=10, n_levels=nl, exact_rrqr=exact)
     S.factorize()
     sigma = S.solve(np.ones(K.N))
-    SO = oracle.AIFMM(O, leaf_size=16, tol_pow=8, fillin_tol=10)
+    SO = oracle.AIFMM(O, leaf_size=16, tol_pow=8, fillin_tol=10, n_levels=nl)
     SO.factorize()
     so = SO.solve(np.ones(K.N))
     assert rel(sigma, so) < PARITY
