@@ -130,6 +130,13 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
 int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int tol_pow1, int tol_pow2,
                        double input_pivot, int fill_rank, int real_mode, void* Q_device, int* rank_device,
                        double* max_pivot_device, void* stream);
+/* C = alpha op(A) op(B) + beta C (complex128 host arrays, column-major;
+ * op: 0 none, 1 conjugate transpose) through the solver's grouped GEMM:
+ * precision 0 = FP64 FMA, 1 = split-TF32 tensor cores with FP32 accumulation
+ * (FP32 accuracy).  The dense products of the reference go through Eigen;
+ * this is the kernel that replaces them on the GPU. */
+int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
+                const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
 /* X = A^{-1} B by partial-pivot LU (Eigen PartialPivLU semantics, as in
  * EFIEMatrix::getCoefficients, src/EFIEMatrix.cpp:831-837). */
 int aifmm_lu_solve(aifmm_ctx* ctx, const double* A, int n, const double* B, int nrhs, double* X);
@@ -141,7 +148,12 @@ typedef struct {
   int fillin_tol;  /* RRQR partition-2 tolerance 10^-fillin_tol */
   int fillin_rank; /* accepted for compatibility; the reference's active path ignores it */
   int n_levels;    /* 0 = the reference's rule max(2, floor(log8(N / leaf))) */
-  int precision;   /* 0 = plain complex128 (the reference's arithmetic) */
+  int precision;   /* 0 = plain complex128 (the reference's arithmetic); 1 = mixed:
+                    * the elimination's dense products (Schur updates, LU trailing
+                    * updates) run on the tensor cores in split TF32 with FP32
+                    * accumulation (FP32 accuracy) while RRQR, pivots, norms and
+                    * solves stay FP64 -- a preconditioner for
+                    * aifmm_solver_solve_gmres */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
                     * Householder pass, as the reference does; 0 (default) skips
                     * that pass when the old basis is one this solver produced with

@@ -55,6 +55,7 @@ SIGNATURES = {
     "aifmm_rrqr": (_i, [_p, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, C.POINTER(_i), C.POINTER(_d)]),
     "aifmm_rrqr_noalloc": (_i, [_p, _i, _i, _i, _i, _i, _d, _i, _i, _p, _p, _p, _p]),
     "aifmm_lu_solve": (_i, [_p, _dp, _i, _dp, _i, _dp]),
+    "aifmm_zgemm": (_i, [_p, _i, _i, _i, _i, _i, _i, _dp, _dp, _i, _dp, _i, _dp, _dp, _i]),
     "aifmm_solver_dump": (_i, [_p, _p, C.c_long, C.POINTER(C.c_long)]),
     "aifmm_operator_create": (_i, [_p, _p, _pp]),
     "aifmm_operator_apply": (_i, [_p, _dp, _i, _dp]),

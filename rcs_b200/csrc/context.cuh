@@ -17,6 +17,7 @@ struct aifmm_ctx {
   cudaMemPool_t pool = nullptr;
   size_t bytes_live = 0;
   int refs = 1;          // the creator's reference
+  int gemmPrecision = 0; // grouped GEMMs: 0 complex128 FMA, 1 split-TF32 tensor cores (FP32 accuracy)
   bool closed = false;
 };
 

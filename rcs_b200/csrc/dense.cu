@@ -10,8 +10,20 @@ namespace aifmm {
 // ------------------------------------------------------------------ GEMM
 constexpr int GBM = 64, GBN = 64, GBK = 8;
 
-struct GemmTile {
-  int prob, tm, tn, pad;
+// A group = a chain of problems accumulated into one C (consecutive in the
+// problem list); its tiles are numbered from tileStart, tilesN along n.
+struct GemmGroup {
+  int head, nchain, tilesN, tileStart;
+};
+// Launch arguments.  Up to GEMM_INLINE groups travel in the kernel's
+// parameter space (no upload); larger launches read device arrays.
+constexpr int GEMM_INLINE = 96;
+struct GemmArgs {
+  int ngroups;
+  const GemmProblem* probs;
+  const GemmGroup* groups;
+  GemmProblem ip[GEMM_INLINE];
+  GemmGroup ig[GEMM_INLINE];
 };
 
 __device__ __forceinline__ zd ldA(const GemmProblem& P, int i, int k) {
@@ -25,24 +37,14 @@ __device__ __forceinline__ zd ldB(const GemmProblem& P, int k, int j) {
   return zconj(P.B[(size_t)k * P.ldb + j]);
 }
 
-__global__ void __launch_bounds__(256) zgemm_grouped_kernel(const GemmProblem* __restrict__ probs,
-                                                            const GemmTile* __restrict__ tiles) {
-  __shared__ zd As[2][GBK][GBM];
-  __shared__ zd Bs[2][GBK][GBN];
-  const GemmTile T = tiles[blockIdx.x];
-  const GemmProblem P = probs[T.prob];
+// acc += op(A) op(B) over the 64x64 tile at (row0, col0); K staged through
+// double-buffered shared slices with register prefetch of the next slice.
+__device__ __forceinline__ void gemm_tile_accumulate(const GemmProblem& P, int row0, int col0, zd (&acc)[4][4],
+                                                     zd (&As)[2][GBK][GBM], zd (&Bs)[2][GBK][GBN]) {
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int row0 = T.tm * GBM, col0 = T.tn * GBN;
-  // load mapping: A tile 64x8 -> thread loads (i = t%64, k = t/64) and (i, k+4)
-  //               B tile 8x64 -> thread loads (k = t%8, j = t/8) and (k, j+32)
   const int t = threadIdx.x;
   const int ai = t & 63, ak = t >> 6;
   const int bk = t & 7, bj = t >> 3;
-  zd acc[4][4];
-#pragma unroll
-  for (int i = 0; i < 4; ++i)
-#pragma unroll
-    for (int j = 0; j < 4; ++j) acc[i][j] = zmk(0, 0);
   zd ra0 = ldA(P, row0 + ai, ak), ra1 = ldA(P, row0 + ai, ak + 4);
   zd rb0 = ldB(P, bk, col0 + bj), rb1 = ldB(P, bk, col0 + bj + 32);
   int buf = 0;
@@ -53,7 +55,7 @@ __global__ void __launch_bounds__(256) zgemm_grouped_kernel(const GemmProblem* _
     Bs[buf][bk][bj + 32] = rb1;
     __syncthreads();
     const int kn = k0 + GBK;
-    if (kn < P.k) {  // prefetch the next K slice while computing this one
+    if (kn < P.k) {
       ra0 = ldA(P, row0 + ai, kn + ak);
       ra1 = ldA(P, row0 + ai, kn + ak + 4);
       rb0 = ldB(P, kn + bk, col0 + bj);
@@ -78,6 +80,33 @@ __global__ void __launch_bounds__(256) zgemm_grouped_kernel(const GemmProblem* _
     }
     buf ^= 1;
   }
+  __syncthreads();  // the next chained problem reuses the shared slices
+}
+
+template <bool INLINE>
+__global__ void __launch_bounds__(256) zgemm_grouped_kernel(const __grid_constant__ GemmArgs a) {
+  __shared__ zd As[2][GBK][GBM];
+  __shared__ zd Bs[2][GBK][GBN];
+  const GemmGroup* G = INLINE ? a.ig : a.groups;
+  const GemmProblem* probs = INLINE ? a.ip : a.probs;
+  int lo = 0, hi = a.ngroups - 1;
+  const int tile = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G[mid].tileStart <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmGroup g = G[lo];
+  const int local = tile - g.tileStart;
+  const int row0 = (local / g.tilesN) * GBM, col0 = (local % g.tilesN) * GBN;
+  zd acc[4][4];
+#pragma unroll
+  for (int i = 0; i < 4; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = zmk(0, 0);
+  for (int q = 0; q < g.nchain; ++q) gemm_tile_accumulate(probs[g.head + q], row0, col0, acc, As, Bs);
+  const GemmProblem& P = probs[g.head];
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
@@ -93,6 +122,173 @@ __global__ void __launch_bounds__(256) zgemm_grouped_kernel(const GemmProblem* _
       *cp = v;
     }
   }
+}
+
+// ------------------------------------------------------------------ GEMM, split TF32
+// Mixed-precision variant of the same grouped/chained GEMM on the tensor
+// cores: every FP64 complex operand is rounded to FP32 and split into a TF32
+// high part and a TF32 remainder, and each real product X Y is formed as
+// Xh Yh + Xh Yl + Xl Yh with FP32 accumulation (~FP32 accuracy, not FP64).
+// The complex product takes 12 m16n8k8 MMAs per k-step:
+//   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br.
+// Tile 64x64 complex, K slices of 16, 8 warps of 32x16; operands staged in
+// shared memory as four TF32 planes (re/im x hi/lo), rows padded to 20 words
+// so the fragment loads hit 32 distinct banks.
+constexpr int TK = 16, TLD = TK + 4;
+
+__device__ __forceinline__ uint32_t tf32_round(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
+  return r;
+}
+__device__ __forceinline__ void tf32_split(double v, uint32_t& hi, uint32_t& lo) {
+  const float f = (float)v;
+  hi = tf32_round(f);
+  lo = tf32_round(f - __uint_as_float(hi));
+}
+__device__ __forceinline__ void mma_tf32(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+  asm volatile(
+      "mma.sync.aligned.m16n8k8.row.col.f32.tf32.tf32.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+      "{%0,%1,%2,%3};"
+      : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+      : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+struct TcSmem {
+  uint32_t A[4][GBM * TLD];  // planes: re hi, re lo, im hi, im lo; [m][k]
+  uint32_t B[4][GBN * TLD];  // same, [n][k]
+};
+
+// Element e (0..1023) of the 64x16 A slice and of the 16x64 B slice: the
+// index mapping follows the operand's contiguous dimension.
+__device__ __forceinline__ void tc_coords_A(const GemmProblem& P, int e, int& m, int& k) {
+  if (P.opA == OP_N) { m = e & 63; k = e >> 6; }
+  else { k = e & 15; m = e >> 4; }
+}
+__device__ __forceinline__ void tc_coords_B(const GemmProblem& P, int e, int& n, int& k) {
+  if (P.opB == OP_N) { k = e & 15; n = e >> 4; }
+  else { n = e & 63; k = e >> 6; }
+}
+
+__device__ __forceinline__ void tc_accumulate(const GemmProblem& P, int row0, int col0, float (&cr)[2][2][4],
+                                              float (&ci)[2][2][4], TcSmem& S) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int g = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  zd ra[4], rb[4];
+  auto fetch = [&](int k0) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int m, k, n, kb;
+      tc_coords_A(P, tid + 256 * q, m, k);
+      ra[q] = ldA(P, row0 + m, k0 + k);
+      tc_coords_B(P, tid + 256 * q, n, kb);
+      rb[q] = ldB(P, k0 + kb, col0 + n);
+    }
+  };
+  fetch(0);
+  for (int k0 = 0; k0 < P.k; k0 += TK) {
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+      int m, k, n, kb;
+      tc_coords_A(P, tid + 256 * q, m, k);
+      tf32_split(ra[q].x, S.A[0][m * TLD + k], S.A[1][m * TLD + k]);
+      tf32_split(ra[q].y, S.A[2][m * TLD + k], S.A[3][m * TLD + k]);
+      tc_coords_B(P, tid + 256 * q, n, kb);
+      tf32_split(rb[q].x, S.B[0][n * TLD + kb], S.B[1][n * TLD + kb]);
+      tf32_split(rb[q].y, S.B[2][n * TLD + kb], S.B[3][n * TLD + kb]);
+    }
+    __syncthreads();
+    if (k0 + TK < P.k) fetch(k0 + TK);
+#pragma unroll
+    for (int ks = 0; ks < TK; ks += 8) {
+      uint32_t a[4][2][4];  // plane, m-tile, fragment
+      uint32_t b[4][2][2];  // plane, n-tile, fragment
+#pragma unroll
+      for (int pl = 0; pl < 4; ++pl) {
+#pragma unroll
+        for (int mi = 0; mi < 2; ++mi) {
+          const uint32_t* base = S.A[pl] + (wm + mi * 16 + g) * TLD + ks + t;
+          a[pl][mi][0] = base[0];
+          a[pl][mi][1] = base[8 * TLD];
+          a[pl][mi][2] = base[4];
+          a[pl][mi][3] = base[8 * TLD + 4];
+        }
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) {
+          const uint32_t* base = S.B[pl] + (wn + ni * 8 + g) * TLD + ks + t;
+          b[pl][ni][0] = base[0];
+          b[pl][ni][1] = base[4];
+        }
+      }
+#pragma unroll
+      for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+        for (int ni = 0; ni < 2; ++ni) {
+          const uint32_t nbh0 = b[2][ni][0] ^ 0x80000000u, nbh1 = b[2][ni][1] ^ 0x80000000u;
+          const uint32_t nbl0 = b[3][ni][0] ^ 0x80000000u, nbl1 = b[3][ni][1] ^ 0x80000000u;
+          // Cr += Ar Br - Ai Bi
+          mma_tf32(cr[mi][ni], a[0][mi], b[0][ni][0], b[0][ni][1]);
+          mma_tf32(cr[mi][ni], a[0][mi], b[1][ni][0], b[1][ni][1]);
+          mma_tf32(cr[mi][ni], a[1][mi], b[0][ni][0], b[0][ni][1]);
+          mma_tf32(cr[mi][ni], a[2][mi], nbh0, nbh1);
+          mma_tf32(cr[mi][ni], a[2][mi], nbl0, nbl1);
+          mma_tf32(cr[mi][ni], a[3][mi], nbh0, nbh1);
+          // Ci += Ar Bi + Ai Br
+          mma_tf32(ci[mi][ni], a[0][mi], b[2][ni][0], b[2][ni][1]);
+          mma_tf32(ci[mi][ni], a[0][mi], b[3][ni][0], b[3][ni][1]);
+          mma_tf32(ci[mi][ni], a[1][mi], b[2][ni][0], b[2][ni][1]);
+          mma_tf32(ci[mi][ni], a[2][mi], b[0][ni][0], b[0][ni][1]);
+          mma_tf32(ci[mi][ni], a[2][mi], b[1][ni][0], b[1][ni][1]);
+          mma_tf32(ci[mi][ni], a[3][mi], b[0][ni][0], b[0][ni][1]);
+        }
+    }
+    __syncthreads();
+  }
+}
+
+template <bool INLINE>
+__global__ void __launch_bounds__(256) zgemm_tf32x3_kernel(const __grid_constant__ GemmArgs a) {
+  __shared__ TcSmem S;
+  const GemmGroup* G = INLINE ? a.ig : a.groups;
+  const GemmProblem* probs = INLINE ? a.ip : a.probs;
+  int lo = 0, hi = a.ngroups - 1;
+  const int tile = blockIdx.x;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (G[mid].tileStart <= tile) lo = mid;
+    else hi = mid - 1;
+  }
+  const GemmGroup g = G[lo];
+  const int local = tile - g.tileStart;
+  const int row0 = (local / g.tilesN) * GBM, col0 = (local % g.tilesN) * GBN;
+  float cr[2][2][4], ci[2][2][4];
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) cr[mi][ni][r] = ci[mi][ni][r] = 0.f;
+  for (int q = 0; q < g.nchain; ++q) tc_accumulate(probs[g.head + q], row0, col0, cr, ci, S);
+  const GemmProblem& P = probs[g.head];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int gr = lane >> 2, t = lane & 3;
+  const int wm = (warp & 1) * 32, wn = (warp >> 1) * 16;
+  const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
+#pragma unroll
+  for (int mi = 0; mi < 2; ++mi)
+#pragma unroll
+    for (int ni = 0; ni < 2; ++ni)
+#pragma unroll
+      for (int r = 0; r < 4; ++r) {
+        const int row = row0 + wm + mi * 16 + gr + ((r & 2) ? 8 : 0);
+        const int col = col0 + wn + ni * 8 + 2 * t + (r & 1);
+        if (row >= P.m || col >= P.n) continue;
+        zd* cp = P.C + (size_t)col * P.ldc + row;
+        zd v = zmul(P.alpha, zmk((double)cr[mi][ni][r], (double)ci[mi][ni][r]));
+        if (!beta0) v = zadd(v, zmul(P.beta, *cp));
+        *cp = v;
+      }
 }
 
 // Optional per-launch timing of the grouped GEMM (events on the launching
@@ -127,49 +323,98 @@ void gemm_profile_read(double* ms, double* flops, long* launches) {
   *launches = g_prof.launches;
 }
 
-void zgemm_grouped(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs) {
+void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
+  AIFMM_REQUIRE(probs.size() == chain.size(), AIFMM_EINVAL, "chain lengths do not match the problems");
   std::vector<GemmProblem> ps;
-  std::vector<GemmTile> tiles;
-  ps.reserve(probs.size());
-  for (const GemmProblem& p : probs) {
-    if (p.m <= 0 || p.n <= 0) continue;
-    if (p.k <= 0) {  // C = beta C
-      if (!(p.beta.x == 1.0 && p.beta.y == 0.0)) {
-        CopyProblem c{p.C, p.C, p.m, p.n, p.ldc, p.ldc, 0, p.beta};
-        zcopy_grouped(ctx, {c});
-      }
-      continue;
+  std::vector<GemmGroup> gs;
+  long tiles = 0;
+  double flops = 0;
+  for (size_t i = 0; i < probs.size();) {
+    const int len = chain[i];
+    AIFMM_REQUIRE(len >= 1 && i + len <= probs.size(), AIFMM_EINVAL, "bad chain length");
+    const GemmProblem& h = probs[i];
+    for (int q = 1; q < len; ++q) {
+      const GemmProblem& p = probs[i + q];
+      AIFMM_REQUIRE(p.C == h.C && p.m == h.m && p.n == h.n && p.ldc == h.ldc && p.alpha.x == h.alpha.x &&
+                        p.alpha.y == h.alpha.y && p.beta.x == 1.0 && p.beta.y == 0.0,
+                    AIFMM_EINVAL, "chained GEMMs must share C, shape and alpha, with beta 1 after the first");
     }
-    const int pi = (int)ps.size();
-    ps.push_back(p);
-    const int tm = (p.m + GBM - 1) / GBM, tn = (p.n + GBN - 1) / GBN;
-    for (int a = 0; a < tm; ++a)
-      for (int b = 0; b < tn; ++b) tiles.push_back({pi, a, b, 0});
+    if (h.m > 0 && h.n > 0) {
+      GemmGroup g;
+      g.head = (int)ps.size();
+      g.nchain = len;
+      g.tilesN = (h.n + GBN - 1) / GBN;
+      g.tileStart = (int)tiles;
+      for (int q = 0; q < len; ++q) {
+        ps.push_back(probs[i + q]);
+        flops += 8.0 * probs[i + q].m * (double)probs[i + q].n * std::max(probs[i + q].k, 0);
+      }
+      gs.push_back(g);
+      tiles += (long)((h.m + GBM - 1) / GBM) * g.tilesN;
+    }
+    i += len;
   }
-  if (tiles.empty()) return;
-  AIFMM_REQUIRE(tiles.size() < (size_t)INT32_MAX, AIFMM_EOVERFLOW, "too many GEMM tiles");
-  DevBuf dp = upload(ctx, ps), dt = upload(ctx, tiles);
+  if (gs.empty()) return;
+  AIFMM_REQUIRE(tiles < (long)INT32_MAX, AIFMM_EOVERFLOW, "too many GEMM tiles");
+  static_assert(sizeof(GemmArgs) < 32000, "GEMM arguments exceed the kernel parameter space");
+  GemmArgs a;
+  a.ngroups = (int)gs.size();
+  a.probs = nullptr;
+  a.groups = nullptr;
+  DevBuf dp, dg;
+  const bool inl = gs.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
+  if (inl) {
+    std::copy(ps.begin(), ps.end(), a.ip);
+    std::copy(gs.begin(), gs.end(), a.ig);
+  } else {
+    dp = upload(ctx, ps);
+    dg = upload(ctx, gs);
+    a.probs = dp.as<GemmProblem>();
+    a.groups = dg.as<GemmGroup>();
+  }
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (g_prof.on) {
     AIFMM_CUDA(cudaEventCreate(&e0));
     AIFMM_CUDA(cudaEventCreate(&e1));
     AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
   }
-  zgemm_grouped_kernel<<<(unsigned)tiles.size(), 256, 0, ctx->stream>>>(dp.as<GemmProblem>(), dt.as<GemmTile>());
+  if (ctx->gemmPrecision == 1) {
+    if (inl) zgemm_tf32x3_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
+    else zgemm_tf32x3_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
+  } else {
+    if (inl) zgemm_grouped_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
+    else zgemm_grouped_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
+  }
   AIFMM_LAUNCHED();
   if (g_prof.on) {
     AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
     g_prof.ev.push_back({e0, e1});
-    for (const GemmProblem& p : ps) g_prof.flops += 8.0 * p.m * (double)p.n * p.k;
+    g_prof.flops += flops;
     g_prof.launches++;
   }
 }
 
+void zgemm_grouped(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs) {
+  zgemm_chained(ctx, probs, std::vector<int>(probs.size(), 1));
+}
+
 // ------------------------------------------------------------------ copies
-__global__ void zcopy_grouped_kernel(const CopyProblem* __restrict__ probs, int nprob, const long* __restrict__ start,
-                                     long total) {
-  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
-    int lo = 0, hi = nprob - 1;
+constexpr int COPY_INLINE = 128;
+struct CopyArgs {
+  int nprob;
+  long total;
+  const CopyProblem* probs;
+  const long* start;
+  CopyProblem ip[COPY_INLINE];
+  long is[COPY_INLINE];
+};
+
+template <bool INLINE>
+__global__ void zcopy_grouped_kernel(const __grid_constant__ CopyArgs a) {
+  const CopyProblem* probs = INLINE ? a.ip : a.probs;
+  const long* start = INLINE ? a.is : a.start;
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < a.total; t += (long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = a.nprob - 1;
     while (lo < hi) {
       int mid = (lo + hi + 1) >> 1;
       if (start[mid] <= t) lo = mid;
@@ -194,9 +439,23 @@ void zcopy_grouped(aifmm_ctx* ctx, const std::vector<CopyProblem>& probs) {
     total += (long)p.rows * p.cols;
   }
   if (ps.empty()) return;
-  DevBuf dp = upload(ctx, ps), ds = upload(ctx, start);
+  static_assert(sizeof(CopyArgs) < 32000, "copy arguments exceed the kernel parameter space");
+  CopyArgs a;
+  a.nprob = (int)ps.size();
+  a.total = total;
+  a.probs = nullptr;
+  a.start = nullptr;
   const int grid = (int)std::min<long>((total + 255) / 256, 148L * 32);
-  zcopy_grouped_kernel<<<grid, 256, 0, ctx->stream>>>(dp.as<CopyProblem>(), (int)ps.size(), ds.as<long>(), total);
+  if (ps.size() <= (size_t)COPY_INLINE) {
+    std::copy(ps.begin(), ps.end(), a.ip);
+    std::copy(start.begin(), start.end(), a.is);
+    zcopy_grouped_kernel<true><<<grid, 256, 0, ctx->stream>>>(a);
+  } else {
+    DevBuf dp = upload(ctx, ps), ds = upload(ctx, start);
+    a.probs = dp.as<CopyProblem>();
+    a.start = ds.as<long>();
+    zcopy_grouped_kernel<false><<<grid, 256, 0, ctx->stream>>>(a);
+  }
   AIFMM_LAUNCHED();
 }
 

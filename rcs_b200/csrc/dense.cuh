@@ -21,8 +21,14 @@ struct GemmProblem {
   zd alpha, beta;
 };
 
-// C = alpha op(A) op(B) + beta C for every problem, one launch.
+// C = alpha op(A) op(B) + beta C for every problem, one launch; the
+// problems must write disjoint C.
 void zgemm_grouped(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs);
+// Same with chains: chain[i] = L > 0 makes problems i..i+L-1 one
+// accumulation C = alpha sum_q op(A_q) op(B_q) + beta_i C (they share C,
+// m, n, ldc and alpha; beta is 1 after the first); chain[i+1..i+L-1] are
+// ignored.  Distinct chains must write disjoint C.
+void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain);
 // Per-launch CUDA-event timing of zgemm_grouped (process-wide switch).
 void gemm_profile_enable(bool on);
 void gemm_profile_read(double* ms, double* flops, long* launches);

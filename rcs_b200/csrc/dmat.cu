@@ -20,15 +20,44 @@ void GemmBatch::add(DMat& C, const DMat& A, int opA, const DMat& B, int opB, zd 
 // read-modify-write of C would race): problem q goes to wave w = number of
 // earlier problems with the same C, and waves run in order, which also keeps
 // the accumulation order of each output equal to the insertion order.
+// Problems with the same C become one chain when they share shape and alpha
+// and every later one has beta 1 (the accumulations the solver issues);
+// otherwise the repeats go to later launches, one wave per repeat.
 void GemmBatch::flush(aifmm_ctx* ctx) {
   if (probs.empty()) return;
-  std::map<const zd*, int> seen;
-  std::vector<std::vector<GemmProblem>> waves;
-  for (const GemmProblem& p : probs) {
-    const int w = seen[p.C]++;
-    if ((int)waves.size() <= w) waves.resize(w + 1);
-    waves[w].push_back(p);
+  std::map<const zd*, std::vector<int>> byC;
+  std::vector<const zd*> order;
+  for (int i = 0; i < (int)probs.size(); ++i) {
+    auto& v = byC[probs[i].C];
+    if (v.empty()) order.push_back(probs[i].C);
+    v.push_back(i);
   }
+  std::vector<GemmProblem> ps;
+  std::vector<int> chain;
+  std::vector<std::vector<GemmProblem>> waves;
+  for (const zd* c : order) {
+    const std::vector<int>& ids = byC[c];
+    const GemmProblem& h = probs[ids[0]];
+    bool ok = true;
+    for (size_t q = 1; q < ids.size() && ok; ++q) {
+      const GemmProblem& p = probs[ids[q]];
+      ok = p.m == h.m && p.n == h.n && p.ldc == h.ldc && p.alpha.x == h.alpha.x && p.alpha.y == h.alpha.y &&
+           p.beta.x == 1.0 && p.beta.y == 0.0;
+    }
+    if (ok) {
+      chain.push_back((int)ids.size());
+      for (size_t q = 1; q < ids.size(); ++q) chain.push_back(0);
+      for (int i : ids) ps.push_back(probs[i]);
+    } else {
+      ps.push_back(h);
+      chain.push_back(1);
+      for (size_t q = 1; q < ids.size(); ++q) {
+        if (waves.size() < q) waves.resize(q);
+        waves[q - 1].push_back(probs[ids[q]]);
+      }
+    }
+  }
+  zgemm_chained(ctx, ps, chain);
   for (auto& w : waves) zgemm_grouped(ctx, w);
   probs.clear();
 }

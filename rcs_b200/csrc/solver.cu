@@ -13,6 +13,14 @@ static double wall() {
 }
 static const zd ONE = {1.0, 0.0}, ZERO = {0.0, 0.0}, MONE = {-1.0, 0.0};
 
+// Grouped GEMMs issued inside the scope use the given precision.
+struct GemmPrecisionScope {
+  aifmm_ctx* c;
+  int saved;
+  GemmPrecisionScope(aifmm_ctx* ctx, int p) : c(ctx), saved(ctx->gemmPrecision) { c->gemmPrecision = p; }
+  ~GemmPrecisionScope() { c->gemmPrecision = saved; }
+};
+
 // Adds the wall time of a scope to a phase counter; with phaseTiming the
 // stream is drained on entry and exit so the time is the phase's own.
 // Nested scopes (RRQR inside a recompression) count in both.
@@ -794,6 +802,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
 // eliminate_x, T:3561-3611 with :3656-3791 (empty box) and :3800-4042.
 void Solver::eliminateX(int j, int k) {
   PhaseTimer pt(*this, stats.t_elim_x);
+  GemmPrecisionScope gp(ctx, prm.precision);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;
@@ -904,6 +913,7 @@ void Solver::eliminateX(int j, int k) {
 // eliminate_z, T:4081-4113 with :4151-4296 (empty) and :4304-4509.
 void Solver::eliminateZ(int j, int k) {
   PhaseTimer pt(*this, stats.t_elim_z);
+  GemmPrecisionScope gp(ctx, prm.precision);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;

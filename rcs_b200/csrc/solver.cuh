@@ -21,6 +21,7 @@ struct SolverParams {
   size_t aca_budget = (size_t)24 << 30;  // bytes of ACA workspace per launch
   bool phaseTiming = false;              // synchronise at phase boundaries for exact phase times
   bool orthoShortcut = true;             // skip partition 1 of RRQR for orthonormal old bases
+  int precision = 0;                     // 1: elimination GEMMs in split TF32 on the tensor cores
 };
 
 struct SolverStats {

@@ -50,6 +50,26 @@ def RRQR(A: np.ndarray, tol_pow1: int, tol_pow2: int, partition: int, input_pivo
     return Q[: 2 * m * k].view(np.complex128).reshape(k, m).T.copy(), mp.value
 
 
+def zgemm(A, B, opA=0, opB=0, alpha=1.0, beta=0.0, C=None, precision=0, ctx=None):
+    """C = alpha op(A) op(B) + beta C on the GPU; op 1 = conjugate transpose;
+    precision 1 = split-TF32 tensor cores (FP32 accuracy)."""
+    ctx = ctx or default_context()
+    A = np.asfortranarray(A, dtype=np.complex128)
+    B = np.asfortranarray(B, dtype=np.complex128)
+    m = A.shape[1] if opA else A.shape[0]
+    k = A.shape[0] if opA else A.shape[1]
+    n = B.shape[0] if opB else B.shape[1]
+    Cm = np.zeros((m, n), dtype=np.complex128, order="F") if C is None else np.array(C, dtype=np.complex128, order="F")
+    al = np.array([complex(alpha).real, complex(alpha).imag])
+    be = np.array([complex(beta).real, complex(beta).imag])
+    cflat = Cm.reshape(-1, order="F")  # a view: Cm is Fortran-ordered
+    _lib.check(_lib.lib().aifmm_zgemm(ctx.h, int(precision), int(opA), int(opB), m, n, k, al,
+                                      A.ravel(order="F").view(np.float64), max(A.shape[0], 1),
+                                      B.ravel(order="F").view(np.float64), max(B.shape[0], 1), be,
+                                      cflat.view(np.float64), max(m, 1)))
+    return Cm
+
+
 def lu_solve(A: np.ndarray, B: np.ndarray, ctx: Context | None = None) -> np.ndarray:
     ctx = ctx or default_context()
     A = np.asarray(A, dtype=np.complex128)

@@ -105,3 +105,21 @@ def test_lu_solve(nrhs):
         B = rng.standard_normal((n, nrhs)) + 1j * rng.standard_normal((n, nrhs))
         X = lowrank.lu_solve(A, B)
         assert np.linalg.norm(A @ X - B) / np.linalg.norm(B) < 1e-10
+
+
+@pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6)])
+@pytest.mark.parametrize("m,n,k,opA,opB", [
+    (64, 64, 16, 0, 0), (1, 1, 1, 0, 0), (65, 33, 17, 1, 0), (200, 130, 451, 0, 1), (37, 300, 5, 1, 1),
+    (10, 10, 0, 0, 0),
+])
+def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
+    """Grouped GEMM in FP64 and in split TF32 (FP32-level accuracy) against numpy."""
+    rng = np.random.default_rng(m * 7 + n * 3 + k)
+    A = rng.standard_normal((k, m) if opA else (m, k)) + 1j * rng.standard_normal((k, m) if opA else (m, k))
+    B = rng.standard_normal((n, k) if opB else (k, n)) + 1j * rng.standard_normal((n, k) if opB else (k, n))
+    C0 = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    alpha, beta = 0.5 - 2j, 1.0 + 0.25j
+    C = lowrank.zgemm(A, B, opA, opB, alpha, beta, C0, precision=precision)
+    ref = alpha * ((A.conj().T if opA else A) @ (B.conj().T if opB else B)) + beta * C0
+    scale = abs(alpha) * np.linalg.norm(A) * np.linalg.norm(B) + abs(beta) * np.linalg.norm(C0)
+    assert np.linalg.norm(C - ref) <= bound * scale

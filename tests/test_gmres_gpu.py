@@ -110,3 +110,21 @@ def test_gmres_zero_rhs_and_bad_arguments():
     A2 = H2Operator(K2, leaf_size=64, tol_pow=8)
     with pytest.raises(AifmmError):  # sizes differ
         S.solve_gmres(A2, np.ones(K.N))
+
+
+def test_mixed_precision_factorization_refines_to_target():
+    """precision=1 (split-TF32 tensor-core elimination GEMMs) as the
+    preconditioner: GMRES reaches 1e-8 against the dense matrix, and the
+    mixed direct solve is no worse than FP32-level noise on top of the plain one."""
+    K = EFIEMatrix(M.icosphere(3, 0.15), 1.0e9)
+    Z = _dense(K)
+    b = K.planeWaveRhs((0, 0, -1), (1, 0, 0))
+    A = H2Operator(K, leaf_size=16, tol_pow=11, n_levels=3)
+    res = {}
+    for prec in (0, 1):
+        S = AIFMM(K, leaf_size=16, tol_pow=6, fillin_tol=8, n_levels=3, precision=prec)
+        S.factorize()
+        res[prec] = np.linalg.norm(Z @ S.solve(b) - b) / np.linalg.norm(b)
+        x, rec = S.solve_gmres(A, b, tol=1e-8)
+        assert np.linalg.norm(Z @ x - b) / np.linalg.norm(b) < 2e-8, (prec, rec)
+    assert res[1] < max(10 * res[0], 1e-5), res
