@@ -132,8 +132,9 @@ int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int to
                        double* max_pivot_device, void* stream);
 /* C = alpha op(A) op(B) + beta C (complex128 host arrays, column-major;
  * op: 0 none, 1 conjugate transpose) through the solver's grouped GEMM:
- * precision 0 = FP64 FMA, 1 = split-TF32 tensor cores with FP32 accumulation
- * (FP32 accuracy).  The dense products of the reference go through Eigen;
+ * precision 0 = FP64 FMA; 1 and 2 = split-TF32 tensor cores with FP32
+ * accumulation (FP32 accuracy): 1 by warp-level mma.sync, 2 by tcgen05 with
+ * tensor-memory accumulators.  The dense products of the reference go through Eigen;
  * this is the kernel that replaces them on the GPU. */
 int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
@@ -239,6 +240,9 @@ int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* r
 int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const void* rhs_device, int nrhs,
                                     void* x_device, double tol, int restart, int maxit, aifmm_gmres_info* info);
 
+/* Number of tcgen05 GEMM tiles whose bounded pipeline wait ran out (their
+ * output was left unwritten); 0 in a healthy run. */
+int aifmm_tc5_timeouts(long* n);
 /* Number of CUDA kernels this library has launched in the process. */
 int aifmm_launch_count(long* n);
 /* Switch per-launch CUDA-event timing of the grouped complex GEMM on (1) or

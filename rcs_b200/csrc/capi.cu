@@ -8,6 +8,7 @@
 
 #include "capi_guard.cuh"
 #include "context.cuh"
+#include "dense.cuh"
 
 namespace aifmm {
 
@@ -67,6 +68,13 @@ using namespace aifmm;
 extern "C" {
 
 const char* aifmm_last_error(void) { return g_last_error.c_str(); }
+
+int aifmm_tc5_timeouts(long* n) {
+  API_BEGIN
+  AIFMM_REQUIRE(n, AIFMM_EINVAL, "NULL argument");
+  *n = zgemm_tc5_timeouts();
+  API_END
+}
 
 int aifmm_launch_count(long* n) {
   if (!n) return AIFMM_EINVAL;

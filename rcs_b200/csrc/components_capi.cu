@@ -117,7 +117,7 @@ int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, i
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc) {
   API_BEGIN
   AIFMM_REQUIRE(ctx && alpha && beta && C && m >= 0 && n >= 0 && k >= 0, AIFMM_EINVAL, "bad argument");
-  AIFMM_REQUIRE(precision == 0 || precision == 1, AIFMM_EINVAL, "precision must be 0 or 1");
+  AIFMM_REQUIRE(precision >= 0 && precision <= 2, AIFMM_EINVAL, "precision must be 0, 1 or 2");
   AIFMM_REQUIRE((opA == 0 || opA == 1) && (opB == 0 || opB == 1), AIFMM_EINVAL, "op must be 0 or 1");
   const int ar = opA ? k : m, ac = opA ? m : k, br = opB ? n : k, bc = opB ? k : n;
   AIFMM_REQUIRE(lda >= std::max(ar, 1) && ldb >= std::max(br, 1) && ldc >= std::max(m, 1), AIFMM_EINVAL,

@@ -17,7 +17,8 @@ struct aifmm_ctx {
   cudaMemPool_t pool = nullptr;
   size_t bytes_live = 0;
   int refs = 1;          // the creator's reference
-  int gemmPrecision = 0; // grouped GEMMs: 0 complex128 FMA, 1 split-TF32 tensor cores (FP32 accuracy)
+  int gemmPrecision = 0; // grouped GEMMs: 0 complex128 FMA; split TF32 (FP32 accuracy) on the tensor
+                         // cores: 1 mma.sync, 2 tcgen05 with tensor-memory accumulators
   bool closed = false;
 };
 

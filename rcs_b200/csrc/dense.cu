@@ -10,22 +10,6 @@ namespace aifmm {
 // ------------------------------------------------------------------ GEMM
 constexpr int GBM = 64, GBN = 64, GBK = 8;
 
-// A group = a chain of problems accumulated into one C (consecutive in the
-// problem list); its tiles are numbered from tileStart, tilesN along n.
-struct GemmGroup {
-  int head, nchain, tilesN, tileStart;
-};
-// Launch arguments.  Up to GEMM_INLINE groups travel in the kernel's
-// parameter space (no upload); larger launches read device arrays.
-constexpr int GEMM_INLINE = 96;
-struct GemmArgs {
-  int ngroups;
-  const GemmProblem* probs;
-  const GemmGroup* groups;
-  GemmProblem ip[GEMM_INLINE];
-  GemmGroup ig[GEMM_INLINE];
-};
-
 __device__ __forceinline__ zd ldA(const GemmProblem& P, int i, int k) {
   if (i >= P.m || k >= P.k) return zmk(0, 0);
   if (P.opA == OP_N) return P.A[(size_t)k * P.lda + i];
@@ -329,6 +313,8 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
   std::vector<GemmGroup> gs;
   long tiles = 0;
   double flops = 0;
+  const int mode = ctx->gemmPrecision;
+  const int bm = (mode == 2) ? 128 : GBM;  // row tile of the tcgen05 kernel
   for (size_t i = 0; i < probs.size();) {
     const int len = chain[i];
     AIFMM_REQUIRE(len >= 1 && i + len <= probs.size(), AIFMM_EINVAL, "bad chain length");
@@ -350,7 +336,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
         flops += 8.0 * probs[i + q].m * (double)probs[i + q].n * std::max(probs[i + q].k, 0);
       }
       gs.push_back(g);
-      tiles += (long)((h.m + GBM - 1) / GBM) * g.tilesN;
+      tiles += (long)((h.m + bm - 1) / bm) * g.tilesN;
     }
     i += len;
   }
@@ -378,7 +364,9 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     AIFMM_CUDA(cudaEventCreate(&e1));
     AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
   }
-  if (ctx->gemmPrecision == 1) {
+  if (mode == 2) {
+    zgemm_tc5_launch(ctx, a, inl, tiles);
+  } else if (mode == 1) {
     if (inl) zgemm_tf32x3_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
     else zgemm_tf32x3_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
   } else {

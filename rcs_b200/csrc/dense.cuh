@@ -21,6 +21,29 @@ struct GemmProblem {
   zd alpha, beta;
 };
 
+// A group = a chain of problems accumulated into one C (consecutive in the
+// problem list); its tiles are numbered from tileStart, tilesN along n.
+struct GemmGroup {
+  int head, nchain, tilesN, tileStart;
+};
+// Launch arguments of the grouped GEMM kernels.  Up to GEMM_INLINE groups
+// travel in the kernel's parameter space (no upload); larger launches read
+// device arrays.
+constexpr int GEMM_INLINE = 96;
+struct GemmArgs {
+  int ngroups;
+  const GemmProblem* probs;
+  const GemmGroup* groups;
+  GemmProblem ip[GEMM_INLINE];
+  GemmGroup ig[GEMM_INLINE];
+};
+// Tensor-core (tcgen05) form of the split-TF32 grouped GEMM, 128x64 complex
+// tiles (zgemm_tc5.cu); groups must be tiled with tilesN = ceil(n / 64) and
+// ceil(m / 128) row tiles.  Returns false when the GPU cannot run it.
+void zgemm_tc5_launch(aifmm_ctx* ctx, const GemmArgs& a, bool inl, long tiles);
+// Number of tcgen05 pipeline waits that ran out (each leaves its tile unwritten).
+long zgemm_tc5_timeouts();
+
 // C = alpha op(A) op(B) + beta C for every problem, one launch; the
 // problems must write disjoint C.
 void zgemm_grouped(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs);
