@@ -154,7 +154,8 @@ typedef struct {
                     * updates) run on the tensor cores in split TF32 with FP32
                     * accumulation (FP32 accuracy) while RRQR, pivots, norms and
                     * solves stay FP64 -- a preconditioner for
-                    * aifmm_solver_solve_gmres */
+                    * aifmm_solver_solve_gmres; 2 = the same with the tcgen05
+                    * kernel (tensor-memory accumulators) instead of mma.sync */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
                     * Householder pass, as the reference does; 0 (default) skips
                     * that pass when the old basis is one this solver produced with

@@ -4,6 +4,7 @@
 #include <chrono>
 #include <cmath>
 
+#include "h2op.cuh"
 #include "solver.cuh"
 
 namespace aifmm {
@@ -1081,21 +1082,35 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
 }
 
 // ------------------------------------------------------------ solve sweeps
+// Tree order of the unknowns: leaves in box order, each leaf's
+// chargeLocations in order; built once, used by the gathers of the sweeps.
+void Solver::treeOrder() {
+  if (leafPermReady_) return;
+  std::vector<int> perm;
+  leafOff_.assign(nBoxesPerLevel[nLevels] + 1, 0);
+  for (int k = 0; k < nBoxesPerLevel[nLevels]; ++k) {
+    leafOff_[k] = (int)perm.size();
+    const auto& cl = tree[nLevels][k].chargeLocations;
+    perm.insert(perm.end(), cl.begin(), cl.end());
+  }
+  leafOff_.back() = (int)perm.size();
+  AIFMM_REQUIRE((int)perm.size() == N, AIFMM_EINVAL, "leaves do not cover every unknown");
+  leafPerm_ = std::make_shared<DevBuf>(upload(ctx, perm));
+  leafPermReady_ = true;
+}
+
 void Solver::assignLeafRhs(const DMat& rhs) {  // T:670-678 (a gather of rows)
   const int j = nLevels;
-  std::vector<int> ids;
+  treeOrder();
+  // rows of rhs in tree order, then one block copy per leaf
+  DMat Xt = ops.alloc(N, nrhs_);
+  zrows_gather(ctx, rhs.p, rhs.ld(), leafPerm_->as<int>(), N, Xt.p, Xt.ld(), nrhs_);
   std::vector<CopyProblem> cps;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
     DBox& B = tree[j][k];
-    B.particle_rhs = ops.alloc((int)B.chargeLocations.size(), nrhs_);
-  }
-  // rows of rhs scattered per box: one copy per unknown would be too many
-  // launches, so gather through a permutation kernel built from copies of
-  // single rows grouped in one launch.
-  for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
-    DBox& B = tree[j][k];
-    for (size_t i = 0; i < B.chargeLocations.size(); ++i)
-      cps.push_back({rhs.p + B.chargeLocations[i], B.particle_rhs.p + i, 1, nrhs_, rhs.ld(), B.particle_rhs.ld(), 0, ONE});
+    const int n = leafOff_[k + 1] - leafOff_[k];
+    B.particle_rhs = ops.alloc(n, nrhs_);
+    if (n > 0) cps.push_back({Xt.p + leafOff_[k], B.particle_rhs.p, n, nrhs_, Xt.ld(), B.particle_rhs.ld(), 0, ONE});
   }
   zcopy_grouped(ctx, cps);
 }
@@ -1237,14 +1252,16 @@ DMat Solver::solve(const DMat& rhs) {
   }
   backSubstitute();
   // getx + reorder (T:4874-4907, :466-476): x[chargeLocations[i]] = particles_i
-  DMat x = ops.zeros(N, nrhs_);
+  DMat Yt = ops.zeros(N, nrhs_);
   std::vector<CopyProblem> cps;
   for (int k = 0; k < nBoxesPerLevel[nLevels]; ++k) {
     DBox& B = tree[nLevels][k];
-    for (size_t i = 0; i < B.chargeLocations.size() && (int)i < B.particles.r; ++i)
-      cps.push_back({B.particles.p + i, x.p + B.chargeLocations[i], 1, nrhs_, B.particles.ld(), x.ld(), 0, ONE});
+    const int n = std::min(leafOff_[k + 1] - leafOff_[k], B.particles.r);
+    if (n > 0) cps.push_back({B.particles.p, Yt.p + leafOff_[k], n, nrhs_, B.particles.ld(), Yt.ld(), 0, ONE});
   }
   zcopy_grouped(ctx, cps);
+  DMat x = ops.alloc(N, nrhs_);
+  zrows_scatter(ctx, Yt.p, Yt.ld(), leafPerm_->as<int>(), N, x.p, x.ld(), nrhs_);
   ops.sync();
   stats.t_solve = wall() - t0;
   return x;

@@ -118,7 +118,11 @@ class Solver {
   void gatherBlocks(const std::vector<std::vector<int>*>& rows, const std::vector<std::vector<int>*>& cols,
                     std::vector<DMat*>& outs);
   std::vector<std::vector<DBox>> deepCopy(std::vector<std::vector<DBox>>& src);
+  void treeOrder();
   int nrhs_ = 1;
+  bool leafPermReady_ = false;
+  std::shared_ptr<DevBuf> leafPerm_;  // tree-order position -> unknown id
+  std::vector<int> leafOff_;          // leaf box -> first tree-order position
   std::vector<std::vector<DBox>> saved_;
   bool hasSaved_ = false;
 };
