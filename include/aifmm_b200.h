@@ -138,6 +138,10 @@ int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int to
  * this is the kernel that replaces them on the GPU. */
 int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
+/* Same with device pointers, asynchronous on the context stream. */
+int aifmm_zgemm_device(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
+                       const void* A_device, int lda, const void* B_device, int ldb, const double beta[2],
+                       void* C_device, int ldc);
 /* X = A^{-1} B by partial-pivot LU (Eigen PartialPivLU semantics, as in
  * EFIEMatrix::getCoefficients, src/EFIEMatrix.cpp:831-837). */
 int aifmm_lu_solve(aifmm_ctx* ctx, const double* A, int n, const double* B, int nrhs, double* X);
@@ -176,6 +180,9 @@ typedef struct {
    * solver then synchronises at every phase boundary), else host-side
    * approximations. */
   double t_rrqr, t_compress, t_elim_x, t_elim_z, t_nonleaf;
+  /* inside eliminate_x/z: box LU factorizations, their multi-column solves,
+   * the Schur-complement GEMM launches */
+  double t_lu, t_msolve, t_schur;
 } aifmm_solver_info;
 
 /* AIFMM<K>::AIFMM(inputsToSolverClass, K*) (src/AIFMM.cpp:7-93): builds the

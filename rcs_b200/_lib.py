@@ -57,6 +57,7 @@ SIGNATURES = {
     "aifmm_rrqr_noalloc": (_i, [_p, _i, _i, _i, _i, _i, _d, _i, _i, _p, _p, _p, _p]),
     "aifmm_lu_solve": (_i, [_p, _dp, _i, _dp, _i, _dp]),
     "aifmm_zgemm": (_i, [_p, _i, _i, _i, _i, _i, _i, _dp, _dp, _i, _dp, _i, _dp, _dp, _i]),
+    "aifmm_zgemm_device": (_i, [_p, _i, _i, _i, _i, _i, _i, _dp, _p, _i, _p, _i, _dp, _p, _i]),
     "aifmm_solver_dump": (_i, [_p, _p, C.c_long, C.POINTER(C.c_long)]),
     "aifmm_operator_create": (_i, [_p, _p, _pp]),
     "aifmm_operator_apply": (_i, [_p, _dp, _i, _dp]),
@@ -83,7 +84,8 @@ class SolverInfo(C.Structure):
                 ("t_factor", C.c_double), ("t_solve", C.c_double), ("flops_factor", C.c_double),
                 ("mem_gb", C.c_double), ("mem_after_gb", C.c_double), ("t_rrqr", C.c_double),
                 ("t_compress", C.c_double), ("t_elim_x", C.c_double), ("t_elim_z", C.c_double),
-                ("t_nonleaf", C.c_double)]
+                ("t_nonleaf", C.c_double), ("t_lu", C.c_double), ("t_msolve", C.c_double),
+                ("t_schur", C.c_double)]
 
 class GmresInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("cycles", C.c_int), ("relres", C.c_double), ("t_precond", C.c_double),

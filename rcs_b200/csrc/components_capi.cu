@@ -113,24 +113,9 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
   API_END
 }
 
-int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
-                const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc) {
-  API_BEGIN
-  AIFMM_REQUIRE(ctx && alpha && beta && C && m >= 0 && n >= 0 && k >= 0, AIFMM_EINVAL, "bad argument");
-  AIFMM_REQUIRE(precision >= 0 && precision <= 2, AIFMM_EINVAL, "precision must be 0, 1 or 2");
-  AIFMM_REQUIRE((opA == 0 || opA == 1) && (opB == 0 || opB == 1), AIFMM_EINVAL, "op must be 0 or 1");
-  const int ar = opA ? k : m, ac = opA ? m : k, br = opB ? n : k, bc = opB ? k : n;
-  AIFMM_REQUIRE(lda >= std::max(ar, 1) && ldb >= std::max(br, 1) && ldc >= std::max(m, 1), AIFMM_EINVAL,
-                "leading dimension too small");
-  AIFMM_REQUIRE(k == 0 || (A && B), AIFMM_EINVAL, "NULL operand");
-  AIFMM_CUDA(cudaSetDevice(ctx->device));
-  const size_t za = (size_t)lda * ac, zb = (size_t)ldb * bc, zc = (size_t)ldc * n;
-  DevBuf dA(ctx, sizeof(zd) * za + 16), dB(ctx, sizeof(zd) * zb + 16), dC(ctx, sizeof(zd) * zc + 16);
-  if (za) AIFMM_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(zd) * za, cudaMemcpyHostToDevice, ctx->stream));
-  if (zb) AIFMM_CUDA(cudaMemcpyAsync(dB.p, B, sizeof(zd) * zb, cudaMemcpyHostToDevice, ctx->stream));
-  if (zc) AIFMM_CUDA(cudaMemcpyAsync(dC.p, C, sizeof(zd) * zc, cudaMemcpyHostToDevice, ctx->stream));
-  GemmProblem g{dA.as<zd>(), dB.as<zd>(), dC.as<zd>(), m, n, k, lda, ldb, ldc, opA, opB, zmk(alpha[0], alpha[1]),
-                zmk(beta[0], beta[1])};
+static void zgemm_checked(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double* alpha,
+                          const zd* A, int lda, const zd* B, int ldb, const double* beta, zd* C, int ldc) {
+  GemmProblem g{A, B, C, m, n, k, lda, ldb, ldc, opA, opB, zmk(alpha[0], alpha[1]), zmk(beta[0], beta[1])};
   const int saved = ctx->gemmPrecision;
   ctx->gemmPrecision = precision;
   try {
@@ -140,8 +125,44 @@ int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, i
     throw;
   }
   ctx->gemmPrecision = saved;
+}
+
+static void zgemm_args(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double* alpha,
+                       const void* A, int lda, const void* B, int ldb, const double* beta, const void* C, int ldc) {
+  AIFMM_REQUIRE(ctx && alpha && beta && C && m >= 0 && n >= 0 && k >= 0, AIFMM_EINVAL, "bad argument");
+  AIFMM_REQUIRE(precision >= 0 && precision <= 2, AIFMM_EINVAL, "precision must be 0, 1 or 2");
+  AIFMM_REQUIRE((opA == 0 || opA == 1) && (opB == 0 || opB == 1), AIFMM_EINVAL, "op must be 0 or 1");
+  const int ar = opA ? k : m, br = opB ? n : k;
+  AIFMM_REQUIRE(lda >= std::max(ar, 1) && ldb >= std::max(br, 1) && ldc >= std::max(m, 1), AIFMM_EINVAL,
+                "leading dimension too small");
+  AIFMM_REQUIRE(k == 0 || (A && B), AIFMM_EINVAL, "NULL operand");
+}
+
+int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
+                const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc) {
+  API_BEGIN
+  zgemm_args(ctx, precision, opA, opB, m, n, k, alpha, A, lda, B, ldb, beta, C, ldc);
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  const int ac = opA ? m : k, bc = opB ? k : n;
+  const size_t za = (size_t)lda * ac, zb = (size_t)ldb * bc, zc = (size_t)ldc * n;
+  DevBuf dA(ctx, sizeof(zd) * za + 16), dB(ctx, sizeof(zd) * zb + 16), dC(ctx, sizeof(zd) * zc + 16);
+  if (za) AIFMM_CUDA(cudaMemcpyAsync(dA.p, A, sizeof(zd) * za, cudaMemcpyHostToDevice, ctx->stream));
+  if (zb) AIFMM_CUDA(cudaMemcpyAsync(dB.p, B, sizeof(zd) * zb, cudaMemcpyHostToDevice, ctx->stream));
+  if (zc) AIFMM_CUDA(cudaMemcpyAsync(dC.p, C, sizeof(zd) * zc, cudaMemcpyHostToDevice, ctx->stream));
+  zgemm_checked(ctx, precision, opA, opB, m, n, k, alpha, dA.as<zd>(), lda, dB.as<zd>(), ldb, beta, dC.as<zd>(), ldc);
   if (zc) AIFMM_CUDA(cudaMemcpyAsync(C, dC.p, sizeof(zd) * zc, cudaMemcpyDeviceToHost, ctx->stream));
   AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  API_END
+}
+
+int aifmm_zgemm_device(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
+                       const void* A_device, int lda, const void* B_device, int ldb, const double beta[2],
+                       void* C_device, int ldc) {
+  API_BEGIN
+  zgemm_args(ctx, precision, opA, opB, m, n, k, alpha, A_device, lda, B_device, ldb, beta, C_device, ldc);
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  zgemm_checked(ctx, precision, opA, opB, m, n, k, alpha, static_cast<const zd*>(A_device), lda,
+                static_cast<const zd*>(B_device), ldb, beta, static_cast<zd*>(C_device), ldc);
   API_END
 }
 

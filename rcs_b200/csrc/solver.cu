@@ -810,7 +810,10 @@ void Solver::eliminateX(int j, int k) {
   for (int nn : B.NB)
     if (nn != k) nbs.push_back(nn);
   if (B.P2P[k].size() != 0) {
-    B.luP2P = ops.factor(B.P2P[k]);
+    {
+      PhaseTimer t(*this, stats.t_lu);
+      B.luP2P = ops.factor(B.P2P[k]);
+    }
     B.hasLuP2P = true;
     const int m = B.P2P[k].r;
     stats.flops_factor += 8.0 / 3.0 * m * (double)m * m;
@@ -825,7 +828,11 @@ void Solver::eliminateX(int j, int k) {
       coff.push_back(tot);
       tot += X.c;
     }
-    DMat W = ops.solve(B.luP2P, ops.hcatv(parts));
+    DMat W;
+    {
+      PhaseTimer t(*this, stats.t_msolve);
+      W = ops.solve(B.luP2P, ops.hcatv(parts));
+    }
     stats.flops_factor += 4.0 * m * (double)m * tot;
     auto Wb = [&](int idx, int cols) {  // column slice view of W
       DMat v;
@@ -881,7 +888,10 @@ void Solver::eliminateX(int j, int k) {
         }
       }
     }
-    g.flush(ctx);
+    {
+      PhaseTimer t(*this, stats.t_schur);
+      g.flush(ctx);
+    }
   } else {
     B.L2M_f = ops.zeros(B.P2M.r, B.L2P.c);
     for (int nn : nbs) {
@@ -922,7 +932,10 @@ void Solver::eliminateZ(int j, int k) {
     if (nn != k) nbs.push_back(nn);
   if (B.L2M_f.size() > 0) {
     AIFMM_REQUIRE(B.L2M_f.r == B.L2M_f.c, AIFMM_EINVAL, "L2M_f is not square");
-    B.luL2M = ops.factor(B.L2M_f);
+    {
+      PhaseTimer t(*this, stats.t_lu);
+      B.luL2M = ops.factor(B.L2M_f);
+    }
     B.hasLuL2M = true;
     const int r = B.L2M_f.r;
     stats.flops_factor += 8.0 / 3.0 * r * (double)r * r;
@@ -936,7 +949,11 @@ void Solver::eliminateZ(int j, int k) {
       coff.push_back(tot);
       tot += X.c;
     }
-    DMat W = ops.solve(B.luL2M, ops.hcatv(parts));
+    DMat W;
+    {
+      PhaseTimer t(*this, stats.t_msolve);
+      W = ops.solve(B.luL2M, ops.hcatv(parts));
+    }
     stats.flops_factor += 4.0 * r * (double)r * tot;
     auto Wb = [&](int idx, int cols) {
       DMat v;
@@ -992,7 +1009,10 @@ void Solver::eliminateZ(int j, int k) {
         }
       }
     }
-    g.flush(ctx);
+    {
+      PhaseTimer t(*this, stats.t_schur);
+      g.flush(ctx);
+    }
     if (!checks.empty()) {  // queue decisions need the norms of the updated blocks (T:4409-4418, :4448-4455)
       std::vector<const DMat*> ms;
       for (auto& c : checks) {
@@ -1041,6 +1061,7 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
   stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
+  stats.t_lu = stats.t_msolve = stats.t_schur = 0;
   for (int j = nLevels; j >= startLevel; --j) {
     if (j != nLevels) {
       initP2PNonLeaf(j);

@@ -27,6 +27,7 @@ struct SolverParams {
 struct SolverStats {
   double t_assemble = 0, t_factor = 0, t_solve = 0;
   double t_rrqr = 0, t_compress = 0, t_elim_x = 0, t_elim_z = 0, t_nonleaf = 0;
+  double t_lu = 0, t_msolve = 0, t_schur = 0;  // inside eliminate_x/z: box LU, multi-column solves, Schur GEMMs
   double flops_factor = 0;  // complex-counted algorithmic flops issued by the factorization
   long nRRQR = 0, nRRQRShort = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
   long kernels = 0;

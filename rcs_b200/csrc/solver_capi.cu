@@ -99,6 +99,9 @@ int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
   info->t_elim_x = S.stats.t_elim_x;
   info->t_elim_z = S.stats.t_elim_z;
   info->t_nonleaf = S.stats.t_nonleaf;
+  info->t_lu = S.stats.t_lu;
+  info->t_msolve = S.stats.t_msolve;
+  info->t_schur = S.stats.t_schur;
   API_END
 }
 
