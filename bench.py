@@ -36,15 +36,16 @@ METRIC = "factor+solve s at rel. residual 1e-6: mixed/batched/learned vs plain F
 # target relative residual (None = direct solve only, the reference's path).
 CONFIGS = {
     "c1": dict(sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0, op_tol=None,
-               gmres=None,
+               gmres=None, precision=0,
                desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10, "
                     "direct solve"),
     "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
-               gmres=1e-6,
+               gmres=1e-6, precision=2,
                desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
-                    "RRQR 1e-7, 8 seeded plane waves, FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
+                    "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs) as the "
+                    "preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
     "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
-                gmres=1e-6,
+                gmres=1e-6, precision=2,
                 desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
                      "8 plane waves, FGMRES(30) to 1e-6 (c3 shape at 1/4 size)"),
 }
@@ -150,7 +151,8 @@ def build_workload(cfg, device: int):
     waves = plane_waves(cfg["nrhs"]) if cfg["nrhs"] > 1 else [(np.array([0.0, 0, -1]), np.array([1, 0, 0j]))]
     B = np.stack([K.planeWaveRhs(k, e) for k, e in waves], axis=1)
     t0 = time.perf_counter()
-    S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"])
+    S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"],
+              precision=cfg.get("precision", 0))
     t_asm = time.perf_counter() - t0
     S.checkpoint()
     A, t_op = None, 0.0
@@ -264,11 +266,12 @@ def run_reference(args, rank, world):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--steps", type=int, default=1)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--config", default=os.environ.get("AIFMM_BENCH_CONFIG", "c3"))
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain FP64 comparison step")
     args = ap.parse_args()
     rank, world, local = dist_env()
     if world > 1:
@@ -358,6 +361,38 @@ def main():
     peak = zgemm_peak_tflops()
     achieved = g_flops / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0
 
+    # the plain FP64 factorization on the same workload and refinement: one
+    # warm-up and one timed step, for the mixed-vs-plain comparison
+    plain = None
+    if cfg.get("precision", 0) != 0 and not args.no_plain:
+        from rcs_b200.solver import AIFMM
+        S0 = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"],
+                   n_levels=cfg["levels"], precision=0)
+        S0.checkpoint()
+        X0 = torch.empty_like(Bd)
+        prec0 = []
+
+        def step0():
+            S0.rewind()
+            S0.factorize()
+            prec0.append(S0.solve_gmres_device(A, Bd.data_ptr(), nrhs, X0.data_ptr(), tol=cfg["gmres"], restart=30,
+                                               maxit=300))
+
+        step0()
+        torch.cuda.synchronize()
+        barrier(world)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        step0()
+        f1.record(stream)
+        torch.cuda.synchronize()
+        t_plain = max_over_ranks(f0.elapsed_time(f1) / 1e3, world)
+        plain = {"value": t_plain, "unit": "s", "steps": 1, "warmup": 1, "gmres_iterations": prec0[-1]["iterations"],
+                 "residual": sampled_residual(K, X0.cpu().numpy().T, B, nrows=512),
+                 "phases_s": {k: S0.info()[k] for k in ("t_rrqr", "t_compress", "t_elim_x", "t_elim_z")},
+                 "speedup_of_value": t_plain / t_step}
+        S0.close()
+
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
@@ -368,15 +403,18 @@ def main():
         line = {
             "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
+            "vs_baseline": None, "dtype": "c128" if cfg.get("precision", 0) == 0 else "c128+tf32x3",
+            "data": "synthetic",
             "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs,
-                       "path": "plain complex128 factorization (reference control flow) + FP64 FGMRES"
-                       if A is not None else "plain complex128 (reference control flow), direct solve",
+                       "path": ({0: "plain complex128 factorization (reference control flow)",
+                                 1: "mixed factorization (split-TF32 mma.sync GEMMs)",
+                                 2: "mixed factorization (split-TF32 tcgen05 GEMMs)"}[cfg.get("precision", 0)]
+                                + (" + FP64 FGMRES" if A is not None else ", direct solve")),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"},
             "residual": res, "residual_e2e": res_e2e, "residual_rows_sampled": min(2048, N),
             "residual_reference": "||Z x - b|| / ||b|| over seeded rows with exact FP64 matrix entries",
-            "gmres": gm, "assemble_s": t_asm, "operator_build_s": t_op,
+            "gmres": gm, "plain_fp64": plain, "assemble_s": t_asm, "operator_build_s": t_op,
             "operator_gb": (A.info()["bytes"] / 1e9) if A is not None else None,
             "factor_flops": info["flops_factor"],
             "phases_s": {k: info[k] for k in ("t_rrqr", "t_compress", "t_elim_x", "t_elim_z", "t_nonleaf")},

@@ -307,6 +307,126 @@ void gemm_profile_read(double* ms, double* flops, long* launches) {
   *launches = g_prof.launches;
 }
 
+// ------------------------------------------------------------------ GEMM, skinny split-K
+// Products with at most 16 columns (the solve sweeps: a box block times a few
+// right-hand sides) are latency-bound in 64x64 tiles: one tile column, the K
+// loop of a whole chain in a handful of CTAs.  Here every (32-row block,
+// problem, 256-column K chunk) is its own CTA writing a partial sum; a second
+// kernel adds each output's partials in a fixed order (deterministic) and
+// applies alpha, beta.
+constexpr int SK_ROWS = 32, SK_KC = 256, SK_NR = 16;
+struct SkItem {
+  int prob, row0, k0, klen, slot;
+};
+struct SkOut {
+  int head, row0, s0, ns;
+};
+
+__global__ void __launch_bounds__(256) zskinny_partial_kernel(const GemmProblem* __restrict__ probs,
+                                                              const SkItem* __restrict__ items, zd* __restrict__ part) {
+  __shared__ zd red[8][8][SK_ROWS];
+  const SkItem it = items[blockIdx.x];
+  const GemmProblem& P = probs[it.prob];
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const int row = it.row0 + lane;
+  const bool live = row < P.m;
+  const int n = P.n;
+  zd acc[SK_NR];
+#pragma unroll
+  for (int r = 0; r < SK_NR; ++r) acc[r] = zmk(0, 0);
+  const zd* A = P.A + (live ? row : 0);
+  const int kend = it.k0 + it.klen;
+#pragma unroll 2
+  for (int k = it.k0 + w; k < kend; k += 8) {
+    const zd a = live ? A[(size_t)k * P.lda] : zmk(0, 0);
+#pragma unroll
+    for (int r = 0; r < SK_NR; ++r)
+      if (r < n) {
+        const zd b = __ldg(P.B + (size_t)r * P.ldb + k);
+        acc[r].x = fma(a.x, b.x, acc[r].x);
+        acc[r].x = fma(-a.y, b.y, acc[r].x);
+        acc[r].y = fma(a.x, b.y, acc[r].y);
+        acc[r].y = fma(a.y, b.x, acc[r].y);
+      }
+  }
+  zd* out = part + (size_t)it.slot * SK_NR * SK_ROWS;
+#pragma unroll
+  for (int half = 0; half < 2; ++half) {
+#pragma unroll
+    for (int r = 0; r < 8; ++r) red[w][r][lane] = acc[half * 8 + r];
+    __syncthreads();
+    const int r = threadIdx.x >> 5, l = threadIdx.x & 31;  // 8 columns x 32 rows
+    zd sum = red[0][r][l];
+#pragma unroll
+    for (int q = 1; q < 8; ++q) sum = zadd(sum, red[q][r][l]);
+    out[(size_t)(half * 8 + r) * SK_ROWS + l] = sum;
+    __syncthreads();
+  }
+}
+
+__global__ void zskinny_reduce_kernel(const GemmProblem* __restrict__ probs, const SkOut* __restrict__ outs,
+                                      const zd* __restrict__ part) {
+  const SkOut o = outs[blockIdx.x];
+  const GemmProblem& P = probs[o.head];
+  const int l = threadIdx.x & 31, r = threadIdx.x >> 5;
+  const int row = o.row0 + l;
+  if (r >= P.n || row >= P.m) return;
+  zd s = zmk(0, 0);
+  for (int i = 0; i < o.ns; ++i) s = zadd(s, part[((size_t)(o.s0 + i) * SK_NR + r) * SK_ROWS + l]);
+  zd* cp = P.C + (size_t)r * P.ldc + row;
+  zd v = zmul(P.alpha, s);
+  if (!(P.beta.x == 0.0 && P.beta.y == 0.0)) v = zadd(v, zmul(P.beta, *cp));
+  *cp = v;
+}
+
+static bool skinny_eligible(const std::vector<GemmProblem>& probs) {
+  bool any = false;
+  for (const GemmProblem& p : probs) {
+    if (p.m <= 0 || p.n <= 0) continue;
+    if (p.n > SK_NR || p.opA != OP_N || p.opB != OP_N) return false;
+    any = true;
+  }
+  return any;
+}
+
+static void zgemm_skinny_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
+  std::vector<GemmProblem> ps;
+  std::vector<SkItem> items;
+  std::vector<SkOut> outs;
+  int slots = 0;
+  for (size_t i = 0; i < probs.size();) {
+    const int len = chain[i];
+    const GemmProblem& h = probs[i];
+    if (h.m > 0 && h.n > 0) {
+      const int head = (int)ps.size();
+      for (int q = 0; q < len; ++q) ps.push_back(probs[i + q]);
+      for (int r0 = 0; r0 < h.m; r0 += SK_ROWS) {
+        SkOut o{head, r0, slots, 0};
+        for (int q = 0; q < len; ++q) {
+          const GemmProblem& p = probs[i + q];
+          for (int k0 = 0; k0 < p.k; k0 += SK_KC) {
+            items.push_back({head + q, r0, k0, std::min(SK_KC, p.k - k0), slots++});
+            o.ns++;
+          }
+        }
+        outs.push_back(o);
+      }
+    }
+    i += len;
+  }
+  if (outs.empty()) return;
+  DevBuf dp = upload(ctx, ps), di = upload(ctx, items), dout = upload(ctx, outs);
+  DevBuf part(ctx, sizeof(zd) * (size_t)std::max(slots, 1) * SK_NR * SK_ROWS);
+  if (!items.empty()) {
+    zskinny_partial_kernel<<<(unsigned)items.size(), 256, 0, ctx->stream>>>(dp.as<GemmProblem>(), di.as<SkItem>(),
+                                                                            part.as<zd>());
+    AIFMM_LAUNCHED();
+  }
+  zskinny_reduce_kernel<<<(unsigned)outs.size(), SK_ROWS * SK_NR, 0, ctx->stream>>>(dp.as<GemmProblem>(),
+                                                                                   dout.as<SkOut>(), part.as<zd>());
+  AIFMM_LAUNCHED();
+}
+
 void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
   AIFMM_REQUIRE(probs.size() == chain.size(), AIFMM_EINVAL, "chain lengths do not match the problems");
   std::vector<GemmProblem> ps;
@@ -341,6 +461,10 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     i += len;
   }
   if (gs.empty()) return;
+  if (skinny_eligible(probs)) {
+    zgemm_skinny_chained(ctx, probs, chain);
+    return;
+  }
   AIFMM_REQUIRE(tiles < (long)INT32_MAX, AIFMM_EOVERFLOW, "too many GEMM tiles");
   static_assert(sizeof(GemmArgs) < 32000, "GEMM arguments exceed the kernel parameter space");
   GemmArgs a;
