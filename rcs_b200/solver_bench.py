@@ -1,0 +1,66 @@
+"""Factor + solve timing of one sphere workload, with the phase breakdown.
+
+    python -m rcs_b200.solver_bench [--sub 4] [--radius 0.15] [--freq 2e9] [--leaf 32]
+                                    [--levels 3] [--tol-pow 5] [--fillin-tol 7]
+                                    [--precision 0|1|2] [--op-tol 10] [--nrhs 8]
+                                    [--gmres 1e-6]
+
+Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
+AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
+times one factorization and one solve (direct, or FGMRES to the target) and
+prints one JSON line with the solver's phase timers.  A small, single-pass
+workload for profiling the whole path (for example under a kernel profiler).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import time
+
+import numpy as np
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--sub", type=int, default=4)
+    ap.add_argument("--radius", type=float, default=0.15)
+    ap.add_argument("--freq", type=float, default=2.0e9)
+    ap.add_argument("--leaf", type=int, default=32)
+    ap.add_argument("--levels", type=int, default=3)
+    ap.add_argument("--tol-pow", type=int, default=5)
+    ap.add_argument("--fillin-tol", type=int, default=7)
+    ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--op-tol", type=int, default=10)
+    ap.add_argument("--nrhs", type=int, default=8)
+    ap.add_argument("--gmres", type=float, default=None)
+    a = ap.parse_args()
+    from . import mesh as M
+    from .kernel import EFIEMatrix
+    from .solver import AIFMM, H2Operator
+    K = EFIEMatrix(M.icosphere(a.sub, a.radius), a.freq)
+    rng = np.random.default_rng(7)
+    B = np.stack([K.planeWaveRhs(d / np.linalg.norm(d), np.cross(d, [0.3, 0.2, 0.9]).astype(complex))
+                  for d in rng.standard_normal((a.nrhs, 3))], axis=1)
+    t0 = time.perf_counter()
+    S = AIFMM(K, leaf_size=a.leaf, tol_pow=a.tol_pow, fillin_tol=a.fillin_tol, n_levels=a.levels,
+              precision=a.precision)
+    t_asm = time.perf_counter() - t0
+    A = H2Operator(K, leaf_size=a.leaf, tol_pow=a.op_tol, n_levels=a.levels) if a.gmres else None
+    t0 = time.perf_counter()
+    S.factorize()
+    t_fac = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    rec = None
+    if A is not None:
+        X, rec = S.solve_gmres(A, B, tol=a.gmres)
+    else:
+        X = S.solve(B)
+    t_sol = time.perf_counter() - t0
+    info = S.info()
+    print(json.dumps({"N": K.N, "precision": a.precision, "assemble_s": t_asm, "factor_s": t_fac, "solve_s": t_sol,
+                      "gmres": rec, "phases_s": {k: v for k, v in info.items() if k.startswith("t_")},
+                      "rrqr": info["n_rrqr"], "flops_factor": info["flops_factor"]}), flush=True)
+
+
+if __name__ == "__main__":
+    main()
