@@ -1,19 +1,20 @@
 // Split-TF32 complex grouped GEMM on the fifth-generation tensor cores
 // (tcgen05): the same chained problem lists as zgemm_grouped, 128x64 complex
-// tiles, one CTA of four warps per tile.
+// tiles, one CTA of eight warps per tile.
 //
-// Each K slice of 8 complex values is staged by all threads: FP64 operands are
-// rounded to FP32 and split into a TF32 high part and a TF32 remainder, real
-// and imaginary parts in separate planes, written in the no-swizzle K-major
-// core-matrix layout (8 rows x 16 bytes per core matrix, K-adjacent cores 128
-// bytes apart, 8-row groups 256 bytes apart).  One thread issues the twelve
-// 128x64x8 MMAs of the slice into two FP32 accumulators in tensor memory
-// (Cr: columns 0..63, Ci: 64..127):
+// Each K slice of 16 complex values (two MMA k-steps of 8) is staged by all
+// threads: FP64 operands are rounded to FP32 and split into a TF32 high part
+// and a TF32 remainder, real and imaginary parts in separate planes, written
+// in the no-swizzle K-major core-matrix layout (8 rows x 16 bytes per core
+// matrix, K-adjacent cores 128 bytes apart, 8-row groups 256 bytes apart).
+// One thread issues the slice's 24 MMAs of 128x64x8 (twelve per k-step) into
+// two FP32 accumulators in tensor memory (Cr: columns 0..63, Ci: 64..127):
 //   Cr += Ar Br - Ai Bi,  Ci += Ar Bi + Ai Br,  each product hi*hi + hi*lo + lo*hi,
 // the subtraction by the instruction's negate-B bit, and commits them to the
 // stage's mbarrier; the slice after next waits on that barrier before reusing
 // the stage (double buffering).  The epilogue reads the accumulators with
-// tcgen05.ld (warp w owns rows 32w..32w+31) and applies alpha, beta in FP64.
+// tcgen05.ld (warp w: rows 32 (w % 4).., columns 32 (w / 4)..) and applies
+// alpha, beta in FP64.
 //
 // Every wait is bounded (one second of GPU time); a wait that runs out leaves
 // its tile unwritten, counts a timeout and waits once more, bounded, for the
@@ -24,14 +25,14 @@
 
 namespace aifmm {
 
-constexpr int C5_M = 128, C5_N = 64, C5_K = 8;
-constexpr int C5_THREADS = 128;
+constexpr int C5_M = 128, C5_N = 64, C5_K = 8, C5_KS = 16;  // MMA k-step, staged slice
+constexpr int C5_THREADS = 256;
 constexpr uint32_t C5_TMEM_COLS = 128;
 constexpr unsigned long long C5_WAIT_NS = 1000000000ull;
 
 struct C5Stage {
-  uint32_t A[4][C5_M * C5_K];  // planes: re hi, re lo, im hi, im lo
-  uint32_t B[4][C5_N * C5_K];
+  uint32_t A[4][C5_KS / C5_K][C5_M * C5_K];  // plane (re hi, re lo, im hi, im lo), k-step, core layout
+  uint32_t B[4][C5_KS / C5_K][C5_N * C5_K];
 };
 struct C5Smem {
   C5Stage st[2];
@@ -121,14 +122,14 @@ __device__ __forceinline__ zd c5_ldB(const GemmProblem& P, int k, int j) {
   if (P.opB == OP_N) return P.B[(size_t)j * P.ldb + k];
   return zconj(P.B[(size_t)k * P.ldb + j]);
 }
-// Element e of the 128x8 A slice / 8x64 B slice, indexed along the operand's
-// contiguous dimension.
+// Element e of the 128x16 A slice / 16x64 B slice, indexed along the
+// operand's contiguous dimension.
 __device__ __forceinline__ void c5_coordA(int opA, int e, int& m, int& k) {
   if (opA == OP_N) { m = e & 127; k = e >> 7; }
-  else { k = e & 7; m = e >> 3; }
+  else { k = e & 15; m = e >> 4; }
 }
 __device__ __forceinline__ void c5_coordB(int opB, int e, int& n, int& k) {
-  if (opB == OP_N) { k = e & 7; n = e >> 3; }
+  if (opB == OP_N) { k = e & 15; n = e >> 4; }
   else { n = e & 63; k = e >> 6; }
 }
 
@@ -172,7 +173,7 @@ __global__ void __launch_bounds__(C5_THREADS, 1) zgemm_tc5_kernel(const __grid_c
   for (int q = 0; q < g.nchain && ok; ++q) {
     const GemmProblem& P = probs[g.head + q];
     if (P.k <= 0) continue;
-    zd ra[8], rb[4];
+    zd ra[8], rb[4];  // 2048 A and 1024 B elements per slice over 256 threads
     auto fetch = [&](int k0) {
 #pragma unroll
       for (int r = 0; r < 8; ++r) {
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(C5_THREADS, 1) zgemm_tc5_kernel(const __grid_c
       }
     };
     fetch(0);
-    for (int k0 = 0; k0 < P.k; k0 += C5_K) {
+    for (int k0 = 0; k0 < P.k; k0 += C5_KS) {
       const int s = it & 1;
       if (it >= 2) {  // the MMAs that read this stage two slices ago must be done
         bool mine = true;
@@ -202,44 +203,49 @@ __global__ void __launch_bounds__(C5_THREADS, 1) zgemm_tc5_kernel(const __grid_c
       for (int r = 0; r < 8; ++r) {
         int m, k;
         c5_coordA(P.opA, tid + C5_THREADS * r, m, k);
-        const int o = c5_off(m, k);
-        c5_split(ra[r].x, st.A[0], st.A[1], o);
-        c5_split(ra[r].y, st.A[2], st.A[3], o);
+        const int ks = k >> 3, o = c5_off(m, k & 7);
+        c5_split(ra[r].x, st.A[0][ks], st.A[1][ks], o);
+        c5_split(ra[r].y, st.A[2][ks], st.A[3][ks], o);
       }
 #pragma unroll
       for (int r = 0; r < 4; ++r) {
         int n, k;
         c5_coordB(P.opB, tid + C5_THREADS * r, n, k);
-        const int o = c5_off(n, k);
-        c5_split(rb[r].x, st.B[0], st.B[1], o);
-        c5_split(rb[r].y, st.B[2], st.B[3], o);
+        const int ks = k >> 3, o = c5_off(n, k & 7);
+        c5_split(rb[r].x, st.B[0][ks], st.B[1][ks], o);
+        c5_split(rb[r].y, st.B[2][ks], st.B[3][ks], o);
       }
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       __syncthreads();
       if (tid == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        const uint64_t dA[4] = {c5_desc(st.A[0]), c5_desc(st.A[1]), c5_desc(st.A[2]), c5_desc(st.A[3])};
-        const uint64_t dB[4] = {c5_desc(st.B[0]), c5_desc(st.B[1]), c5_desc(st.B[2]), c5_desc(st.B[3])};
         constexpr uint32_t ip = c5_idesc(false), in = c5_idesc(true);
         const uint32_t dr = tmem, di = tmem + C5_N;
-        // Cr += Ar Br - Ai Bi
-        c5_mma(dr, dA[0], dB[0], ip, crInit ? 1u : 0u);
-        c5_mma(dr, dA[0], dB[1], ip, 1u);
-        c5_mma(dr, dA[1], dB[0], ip, 1u);
-        c5_mma(dr, dA[2], dB[2], in, 1u);
-        c5_mma(dr, dA[2], dB[3], in, 1u);
-        c5_mma(dr, dA[3], dB[2], in, 1u);
-        // Ci += Ar Bi + Ai Br
-        c5_mma(di, dA[0], dB[2], ip, ciInit ? 1u : 0u);
-        c5_mma(di, dA[0], dB[3], ip, 1u);
-        c5_mma(di, dA[1], dB[2], ip, 1u);
-        c5_mma(di, dA[2], dB[0], ip, 1u);
-        c5_mma(di, dA[2], dB[1], ip, 1u);
-        c5_mma(di, dA[3], dB[0], ip, 1u);
+#pragma unroll
+        for (int ks = 0; ks < C5_KS / C5_K; ++ks) {
+          const uint64_t dA[4] = {c5_desc(st.A[0][ks]), c5_desc(st.A[1][ks]), c5_desc(st.A[2][ks]),
+                                  c5_desc(st.A[3][ks])};
+          const uint64_t dB[4] = {c5_desc(st.B[0][ks]), c5_desc(st.B[1][ks]), c5_desc(st.B[2][ks]),
+                                  c5_desc(st.B[3][ks])};
+          // Cr += Ar Br - Ai Bi
+          c5_mma(dr, dA[0], dB[0], ip, (crInit || ks) ? 1u : 0u);
+          c5_mma(dr, dA[0], dB[1], ip, 1u);
+          c5_mma(dr, dA[1], dB[0], ip, 1u);
+          c5_mma(dr, dA[2], dB[2], in, 1u);
+          c5_mma(dr, dA[2], dB[3], in, 1u);
+          c5_mma(dr, dA[3], dB[2], in, 1u);
+          // Ci += Ar Bi + Ai Br
+          c5_mma(di, dA[0], dB[2], ip, (ciInit || ks) ? 1u : 0u);
+          c5_mma(di, dA[0], dB[3], ip, 1u);
+          c5_mma(di, dA[1], dB[2], ip, 1u);
+          c5_mma(di, dA[2], dB[0], ip, 1u);
+          c5_mma(di, dA[2], dB[1], ip, 1u);
+          c5_mma(di, dA[3], dB[0], ip, 1u);
+        }
         c5_commit(&S.bar[s]);
       }
       crInit = ciInit = true;
-      if (k0 + C5_K < P.k) fetch(k0 + C5_K);
+      if (k0 + C5_KS < P.k) fetch(k0 + C5_KS);
       ++it;
     }
   }
@@ -252,12 +258,15 @@ __global__ void __launch_bounds__(C5_THREADS, 1) zgemm_tc5_kernel(const __grid_c
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
   const GemmProblem& P = probs[g.head];
   if (ok) {
-    const int row = row0 + warp * 32 + lane;
+    // warp w reads tensor-memory lanes 32 (w % 4) .. +31 (its rows) and columns
+    // 32 (w / 4) .. +31 of both accumulators
+    const int quarter = warp & 3, half = warp >> 2;
+    const int row = row0 + quarter * 32 + lane;
     const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
-    for (int c0 = 0; c0 < C5_N; c0 += 16) {
+    for (int c0 = half * 32; c0 < half * 32 + 32; c0 += 16) {
       uint32_t vr[16], vi[16];
       if (it > 0) {
-        const uint32_t ta = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+        const uint32_t ta = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)c0;
         asm volatile(
             "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
             : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]), "=r"(vr[7]),
