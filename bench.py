@@ -364,8 +364,11 @@ def main():
     # the plain FP64 factorization on the same workload and refinement: one
     # warm-up and one timed step, for the mixed-vs-plain comparison
     plain = None
+    info = S.info()
     if cfg.get("precision", 0) != 0 and not args.no_plain:
         from rcs_b200.solver import AIFMM
+        S.close()  # the mixed solver's blocks make room for the plain one
+        torch.cuda.empty_cache()
         S0 = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"],
                    n_levels=cfg["levels"], precision=0)
         S0.checkpoint()

@@ -248,6 +248,13 @@ int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* r
 int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const void* rhs_device, int nrhs,
                                     void* x_device, double tol, int restart, int maxit, aifmm_gmres_info* info);
 
+/* Per-operation accounting of the solver's host-driven factorization and
+ * solve (diagnosis only): on = 1 clears and starts it -- every accounted
+ * operation then synchronises the stream when it ends -- and on = 0 stops it.
+ * The report is text, one line per operation: name, calls, seconds; it is
+ * truncated to cap bytes. */
+int aifmm_profile_ops(int on);
+int aifmm_profile_ops_read(char* buf, int cap);
 /* Number of tcgen05 GEMM tiles whose bounded pipeline wait ran out (their
  * output was left unwritten); 0 in a healthy run. */
 int aifmm_tc5_timeouts(long* n);

@@ -9,6 +9,7 @@
 #include "capi_guard.cuh"
 #include "context.cuh"
 #include "dense.cuh"
+#include "dmat.cuh"
 
 namespace aifmm {
 
@@ -44,6 +45,13 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   ctx = c;
   bytes = n;
   cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
+  if (e == cudaErrorMemoryAllocation) {
+    // the pool keeps freed blocks; return them to the device and retry once
+    cudaGetLastError();
+    cudaStreamSynchronize(c->stream);
+    cudaMemPoolTrimTo(c->pool, 0);
+    e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
+  }
   if (e != cudaSuccess) {
     p = nullptr;
     cudaGetLastError();
@@ -68,6 +76,22 @@ using namespace aifmm;
 extern "C" {
 
 const char* aifmm_last_error(void) { return g_last_error.c_str(); }
+
+int aifmm_profile_ops(int on) {
+  API_BEGIN
+  opprof::enable(on != 0);
+  API_END
+}
+
+int aifmm_profile_ops_read(char* buf, int cap) {
+  API_BEGIN
+  AIFMM_REQUIRE(buf && cap > 0, AIFMM_EINVAL, "bad buffer");
+  const std::string r = opprof::report();
+  const size_t n = std::min(r.size(), (size_t)cap - 1);
+  std::memcpy(buf, r.data(), n);
+  buf[n] = 0;
+  API_END
+}
 
 int aifmm_tc5_timeouts(long* n) {
   API_BEGIN

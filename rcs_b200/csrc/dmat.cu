@@ -1,8 +1,48 @@
 #include "dmat.cuh"
 
+#include <chrono>
+#include <cstdio>
 #include <map>
+#include <mutex>
 
 namespace aifmm {
+
+namespace opprof {
+static bool g_on = false;
+static std::mutex g_mu;
+static std::map<std::string, std::pair<long, double>> g_table;
+static double now() {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+void enable(bool on) {
+  std::lock_guard<std::mutex> l(g_mu);
+  g_on = on;
+  g_table.clear();
+}
+bool enabled() { return g_on; }
+void add(const char* name, double seconds) {
+  std::lock_guard<std::mutex> l(g_mu);
+  auto& e = g_table[name];
+  e.first++;
+  e.second += seconds;
+}
+std::string report() {
+  std::lock_guard<std::mutex> l(g_mu);
+  std::string out;
+  char line[160];
+  for (auto& kv : g_table) {
+    snprintf(line, sizeof(line), "%-24s %10ld %12.6f\n", kv.first.c_str(), kv.second.first, kv.second.second);
+    out += line;
+  }
+  return out;
+}
+Scope::Scope(const char* n, cudaStream_t s) : name(n), stream(s), t0(g_on ? now() : 0.0) {}
+Scope::~Scope() {
+  if (!g_on) return;
+  cudaStreamSynchronize(stream);
+  add(name, now() - t0);
+}
+}  // namespace opprof
 
 void GemmBatch::add(DMat& C, const DMat& A, int opA, const DMat& B, int opB, zd alpha, zd beta) {
   const int m = opA == OP_N ? A.r : A.c;
@@ -24,6 +64,7 @@ void GemmBatch::add(DMat& C, const DMat& A, int opA, const DMat& B, int opB, zd 
 // and every later one has beta 1 (the accumulations the solver issues);
 // otherwise the repeats go to later launches, one wave per repeat.
 void GemmBatch::flush(aifmm_ctx* ctx) {
+  opprof::Scope prof_("gemm_flush", ctx->stream);
   if (probs.empty()) return;
   std::map<const zd*, std::vector<int>> byC;
   std::vector<const zd*> order;
@@ -63,6 +104,7 @@ void GemmBatch::flush(aifmm_ctx* ctx) {
 }
 
 DMat Ops::alloc(int r, int c) const {
+  opprof::Scope prof_("alloc", ctx->stream);
   AIFMM_REQUIRE(r >= 0 && c >= 0, AIFMM_EINVAL, "negative matrix size");
   DMat m;
   m.r = r;
@@ -74,6 +116,7 @@ DMat Ops::alloc(int r, int c) const {
   return m;
 }
 DMat Ops::zeros(int r, int c) const {
+  opprof::Scope prof_("zeros", ctx->stream);
   DMat m = alloc(r, c);
   if (m.size()) AIFMM_CUDA(cudaMemsetAsync(m.p, 0, sizeof(zd) * m.size(), ctx->stream));
   return m;
@@ -84,11 +127,13 @@ DMat Ops::ident(int n, zd d) const {
   return m;
 }
 DMat Ops::copy(const DMat& a) const {
+  opprof::Scope prof_("copy", ctx->stream);
   DMat m = alloc(a.r, a.c);
   if (m.size()) AIFMM_CUDA(cudaMemcpyAsync(m.p, a.p, sizeof(zd) * m.size(), cudaMemcpyDeviceToDevice, ctx->stream));
   return m;
 }
 DMat Ops::block(const DMat& a, int i0, int j0, int nr, int nc) const {
+  opprof::Scope prof_("block", ctx->stream);
   AIFMM_REQUIRE(i0 >= 0 && j0 >= 0 && nr >= 0 && nc >= 0 && i0 + nr <= a.r && j0 + nc <= a.c, AIFMM_EINVAL,
                 "block out of range");
   DMat m = alloc(nr, nc);
@@ -96,6 +141,7 @@ DMat Ops::block(const DMat& a, int i0, int j0, int nr, int nc) const {
   return m;
 }
 DMat Ops::adj(const DMat& a) const {
+  opprof::Scope prof_("adj", ctx->stream);
   DMat m = alloc(a.c, a.r);
   if (m.size()) zcopy_grouped(ctx, {{a.p, m.p, a.c, a.r, a.ld(), m.ld(), 1, zmk(1, 0)}});
   return m;
@@ -112,6 +158,7 @@ void Ops::setBlock(DMat& dst, int i0, int j0, const DMat& src) const {
 }
 DMat Ops::hcat(const DMat& a, const DMat& b) const { return hcatv({a, b}); }
 DMat Ops::hcatv(const std::vector<DMat>& parts) const {
+  opprof::Scope prof_("hcat", ctx->stream);
   int r = parts.empty() ? 0 : parts[0].r, c = 0;
   for (const DMat& q : parts) {
     AIFMM_REQUIRE(q.r == r, AIFMM_EINVAL, "hcat rows mismatch");
@@ -128,6 +175,7 @@ DMat Ops::hcatv(const std::vector<DMat>& parts) const {
   return m;
 }
 DMat Ops::vcat(const std::vector<DMat>& parts) const {
+  opprof::Scope prof_("vcat", ctx->stream);
   int r = 0, c = parts.empty() ? 0 : parts[0].c;
   for (const DMat& q : parts) {
     AIFMM_REQUIRE(q.c == c, AIFMM_EINVAL, "vcat cols mismatch");
@@ -158,6 +206,7 @@ DMat Ops::mul(const DMat& a, int opA, const DMat& b, int opB, zd alpha) const {
   return c;
 }
 std::vector<double> Ops::norms(const std::vector<const DMat*>& ms) const {
+  opprof::Scope prof_("norms", ctx->stream);
   std::vector<double> out(ms.size(), 0.0);
   std::vector<NormProblem> ps;
   std::vector<int> idx;
@@ -189,6 +238,7 @@ double Ops::maxColNorm(const DMat& a) const {
   return best;
 }
 DLU Ops::factor(const DMat& a) const {
+  opprof::Scope prof_("lu_factor", ctx->stream);
   AIFMM_REQUIRE(a.r == a.c, AIFMM_EINVAL, "LU of a non-square matrix");
   DLU f;
   f.n = a.r;
@@ -199,6 +249,7 @@ DLU Ops::factor(const DMat& a) const {
   return f;
 }
 DMat Ops::solve(const DLU& f, const DMat& b) const {
+  opprof::Scope prof_("lu_solve", ctx->stream);
   AIFMM_REQUIRE(b.r == f.n, AIFMM_EINVAL, "LU solve size mismatch");
   DMat x = copy(b);
   if (x.size()) zgetrs(ctx, f.lu.p, f.n, f.lu.ld(), f.piv->as<int>(), x.p, x.c, x.ld());

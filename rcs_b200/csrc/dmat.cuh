@@ -3,11 +3,29 @@
 // shapes, ids and pointers.
 #pragma once
 #include <memory>
+#include <string>
 #include <vector>
 
 #include "dense.cuh"
 
 namespace aifmm {
+
+// Per-operation accounting of the host-driven factorization, for diagnosis:
+// off by default; when on, each instrumented scope synchronises the stream
+// on exit, so its time is host enqueue + device execution of that operation.
+namespace opprof {
+void enable(bool on);
+bool enabled();
+void add(const char* name, double seconds);
+std::string report();
+struct Scope {
+  const char* name;
+  cudaStream_t stream;
+  double t0;
+  Scope(const char* n, cudaStream_t s);
+  ~Scope();
+};
+}  // namespace opprof
 
 struct DMat {
   std::shared_ptr<DevBuf> buf;

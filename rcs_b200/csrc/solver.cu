@@ -526,6 +526,7 @@ bool Solver::wellSeparated(int j, int k, int l) const {  // T:4044-4055
 // Partitioned column-pivoted QR of the working copy R (destroyed); returns
 // Q_trunc.  p2cap bounds the partition-2 steps (-1: none).
 DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot) {
+  opprof::Scope prof_("rrqr_kernels", ctx->stream);
   const int m = R.r, n = R.c;
   const int hs = std::min(m, n) + 1;
   DevBuf H(ctx, sizeof(zd) * (size_t)m * hs + 16), Q(ctx, sizeof(zd) * (size_t)m * hs + 16);
@@ -607,6 +608,7 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
 }
 
 void Solver::updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P) {  // T:3159-3188
+  opprof::Scope prof_("upd_m2l_k", ctx->stream);
   DBox& B = tree[j][k];
   const DMat T = ops.mul(nL2P, OP_C, B.L2P, OP_N);
   GemmBatch g;
@@ -628,6 +630,7 @@ void Solver::updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P) {  // T:3
 }
 
 void Solver::updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt) {  // T:3252-3288
+  opprof::Scope prof_("upd_m2l_b", ctx->stream);
   DBox& Bb = tree[j][b];
   const DMat S = ops.mul(Bb.P2M, OP_N, nP2Mt, OP_N);
   GemmBatch g;
@@ -649,6 +652,7 @@ void Solver::updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt) {  // T:
 }
 
 void Solver::updateParentL2P(int j, int k, const DMat& nL2P) {  // T:3290-3314
+  opprof::Scope prof_("upd_parent_l2p", ctx->stream);
   const int kP = k / nChild, c_k = k % nChild;
   DMat& PL = tree[j - 1][kP].L2P;
   std::vector<DMat> U(nChild);
@@ -663,6 +667,7 @@ void Solver::updateParentL2P(int j, int k, const DMat& nL2P) {  // T:3290-3314
 }
 
 void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt) {  // T:3316-3340
+  opprof::Scope prof_("upd_parent_p2m", ctx->stream);
   const int bP = b / nChild, c_b = b % nChild;
   DMat& PM = tree[j - 1][bP].P2M;
   std::vector<DMat> V(nChild);

@@ -196,6 +196,17 @@ def launch_count() -> int:
     return n.value
 
 
+def profile_ops(on: bool) -> None:
+    """Start (clear) or stop the per-operation accounting of the solver."""
+    _lib.check(_lib.lib().aifmm_profile_ops(int(bool(on))))
+
+
+def profile_ops_read() -> str:
+    buf = C.create_string_buffer(1 << 16)
+    _lib.check(_lib.lib().aifmm_profile_ops_read(buf, len(buf)))
+    return buf.value.decode()
+
+
 def profile_gemm(on: bool) -> None:
     _lib.check(_lib.lib().aifmm_profile_gemm(int(bool(on))))
 
