@@ -154,10 +154,10 @@ typedef struct {
   int fillin_rank; /* accepted for compatibility; the reference's active path ignores it */
   int n_levels;    /* 0 = the reference's rule max(2, floor(log8(N / leaf))) */
   int precision;   /* 0 = plain complex128 (the reference's arithmetic); 1 = mixed:
-                    * the elimination's dense products (Schur updates, LU trailing
-                    * updates) run on the tensor cores in split TF32 with FP32
-                    * accumulation (FP32 accuracy) while RRQR, pivots, norms and
-                    * solves stay FP64 -- a preconditioner for
+                    * the elimination's Schur-complement products run on the
+                    * tensor cores in split TF32 with FP32 accumulation (about
+                    * 1e-5 relative at K = 2048) while the box LU factors, RRQR,
+                    * pivots, norms and solves stay FP64 -- a preconditioner for
                     * aifmm_solver_solve_gmres; 2 = the same with the tcgen05
                     * kernel (tensor-memory accumulators) instead of mma.sync */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1

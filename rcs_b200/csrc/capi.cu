@@ -35,6 +35,10 @@ void ctx_release(aifmm_ctx* c) {
   if (!last) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
+    if (c->ringEvent[i]) cudaEventDestroy(c->ringEvent[i]);
+  if (c->ring) cudaFreeHost(c->ring);
   if (c->pool) cudaMemPoolDestroy(c->pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
@@ -59,6 +63,29 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   }
   c->bytes_live += n;
 }
+void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
+  if (n == 0) return;
+  if (!c->ring || n > aifmm_ctx::kRingBytes / 4) {
+    AIFMM_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, c->stream));
+    return;
+  }
+  size_t head = (c->ringHead + 255) & ~(size_t)255;
+  if (head + n > aifmm_ctx::kRingBytes) {
+    head = 0;
+    c->ringLap++;
+  }
+  const int c0 = (int)(head / aifmm_ctx::kRingChunk), c1 = (int)((head + n - 1) / aifmm_ctx::kRingChunk);
+  for (int q = c0; q <= c1; ++q)  // a chunk from an earlier lap: its last copy must be done
+    if (c->ringChunkLap[q] != 0 && c->ringChunkLap[q] != c->ringLap) AIFMM_CUDA(cudaEventSynchronize(c->ringEvent[q]));
+  std::memcpy(c->ring + head, src, n);
+  AIFMM_CUDA(cudaMemcpyAsync(dst, c->ring + head, n, cudaMemcpyHostToDevice, c->stream));
+  for (int q = c0; q <= c1; ++q) {
+    AIFMM_CUDA(cudaEventRecord(c->ringEvent[q], c->stream));
+    c->ringChunkLap[q] = c->ringLap;
+  }
+  c->ringHead = head + n;
+}
+
 void DevBuf::release() {
   if (p && ctx) {
     cudaFreeAsync(p, ctx->stream);
@@ -123,6 +150,9 @@ int aifmm_ctx_create(int device, aifmm_ctx** out) {
   AIFMM_CUDA(cudaMemPoolCreate(&c->pool, &props));
   uint64_t thresh = UINT64_MAX;  // keep freed blocks for reuse
   AIFMM_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
+  AIFMM_CUDA(cudaMallocHost((void**)&c->ring, aifmm_ctx::kRingBytes));
+  for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
+    AIFMM_CUDA(cudaEventCreateWithFlags(&c->ringEvent[i], cudaEventDisableTiming));
   *out = c.release();
   API_END
 }

@@ -19,6 +19,18 @@ struct aifmm_ctx {
   int refs = 1;          // the creator's reference
   int gemmPrecision = 0; // grouped GEMMs: 0 complex128 FMA; split TF32 (FP32 accuracy) on the tensor
                          // cores: 1 mma.sync, 2 tcgen05 with tensor-memory accumulators
+  // Pinned staging ring for the small host-to-device uploads (problem lists,
+  // index arrays): a copy from pinned memory is asynchronous, one from
+  // pageable memory is not.  Each chunk remembers the event of its last copy
+  // and the lap of the ring it was written in; a chunk written in an earlier
+  // lap is reused only after that copy completed.
+  static constexpr size_t kRingBytes = (size_t)32 << 20, kRingChunk = (size_t)512 << 10;
+  static constexpr int kRingChunks = (int)(kRingBytes / kRingChunk);
+  char* ring = nullptr;
+  size_t ringHead = 0;
+  long ringLap = 1;
+  cudaEvent_t ringEvent[kRingChunks] = {};
+  long ringChunkLap[kRingChunks] = {};  // 0: never used
   bool closed = false;
 };
 
@@ -54,10 +66,14 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
+// Asynchronous host-to-device copy of n bytes on the context stream, staged
+// through the pinned ring when it fits (see aifmm_ctx).
+void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n);
+
 template <typename T>
 DevBuf upload(aifmm_ctx* c, const std::vector<T>& v) {
   DevBuf b(c, std::max<size_t>(1, v.size() * sizeof(T)));
-  if (!v.empty()) AIFMM_CUDA(cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, c->stream));
+  if (!v.empty()) upload_bytes(c, b.p, v.data(), v.size() * sizeof(T));
   return b;
 }
 

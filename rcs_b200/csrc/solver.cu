@@ -808,7 +808,6 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
 // eliminate_x, T:3561-3611 with :3656-3791 (empty box) and :3800-4042.
 void Solver::eliminateX(int j, int k) {
   PhaseTimer pt(*this, stats.t_elim_x);
-  GemmPrecisionScope gp(ctx, prm.precision);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;
@@ -895,6 +894,7 @@ void Solver::eliminateX(int j, int k) {
     }
     {
       PhaseTimer t(*this, stats.t_schur);
+      GemmPrecisionScope gp(ctx, prm.precision);  // the mixed path's tensor-core products
       g.flush(ctx);
     }
   } else {
@@ -929,7 +929,6 @@ void Solver::eliminateX(int j, int k) {
 // eliminate_z, T:4081-4113 with :4151-4296 (empty) and :4304-4509.
 void Solver::eliminateZ(int j, int k) {
   PhaseTimer pt(*this, stats.t_elim_z);
-  GemmPrecisionScope gp(ctx, prm.precision);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
   std::vector<int> nbs;
@@ -1016,6 +1015,7 @@ void Solver::eliminateZ(int j, int k) {
     }
     {
       PhaseTimer t(*this, stats.t_schur);
+      GemmPrecisionScope gp(ctx, prm.precision);  // the mixed path's tensor-core products
       g.flush(ctx);
     }
     if (!checks.empty()) {  // queue decisions need the norms of the updated blocks (T:4409-4418, :4448-4455)

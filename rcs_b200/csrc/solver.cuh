@@ -18,7 +18,7 @@ namespace aifmm {
 struct SolverParams {
   int leafSize = 64, tol_pow = 8, nLevelsInput = 0, fillin_rank = 0, fillin_tol = 10;
   int realMode = 0;      // electrostatics: real Householder sign in RRQR
-  size_t aca_budget = (size_t)8 << 30;   // bytes of ACA workspace per launch
+  size_t aca_budget = (size_t)24 << 30;  // bytes of ACA workspace per launch
   bool phaseTiming = false;              // synchronise at phase boundaries for exact phase times
   bool orthoShortcut = true;             // skip partition 1 of RRQR for orthonormal old bases
   int precision = 0;                     // 1: elimination GEMMs in split TF32 on the tensor cores
