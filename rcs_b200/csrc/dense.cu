@@ -68,7 +68,7 @@ __device__ __forceinline__ void gemm_tile_accumulate(const GemmProblem& P, int r
 }
 
 template <bool INLINE>
-__global__ void __launch_bounds__(256) zgemm_grouped_kernel(const __grid_constant__ GemmArgs a) {
+__global__ void __launch_bounds__(256, 2) zgemm_grouped_kernel(const __grid_constant__ GemmArgs a) {
   __shared__ zd As[2][GBK][GBM];
   __shared__ zd Bs[2][GBK][GBN];
   const GemmGroup* G = INLINE ? a.ig : a.groups;

@@ -122,15 +122,19 @@ __device__ __forceinline__ zd c5_ldB(const GemmProblem& P, int k, int j) {
   if (P.opB == OP_N) return P.B[(size_t)j * P.ldb + k];
   return zconj(P.B[(size_t)k * P.ldb + j]);
 }
-// Element e of the 128x16 A slice / 16x64 B slice, indexed along the
-// operand's contiguous dimension.
+// Element e of the 128x16 A slice / 16x64 B slice.  A warp covers 8 rows x 4
+// k values of one core-matrix group, so its 32 shared-memory stores hit 32
+// distinct banks (word (row % 8) * 4 + k % 4); along the operand's contiguous
+// dimension it reads runs of 8 (m or n) or 4 (k) complex values.
 __device__ __forceinline__ void c5_coordA(int opA, int e, int& m, int& k) {
-  if (opA == OP_N) { m = e & 127; k = e >> 7; }
-  else { k = e & 15; m = e >> 4; }
+  const int lane = e & 31, wid = e >> 5;  // wid: 0..63
+  if (opA == OP_N) { m = (wid & 15) * 8 + (lane & 7); k = (wid >> 4) * 4 + (lane >> 3); }
+  else { m = (wid & 15) * 8 + (lane >> 2); k = (wid >> 4) * 4 + (lane & 3); }
 }
 __device__ __forceinline__ void c5_coordB(int opB, int e, int& n, int& k) {
-  if (opB == OP_N) { k = e & 15; n = e >> 4; }
-  else { n = e & 63; k = e >> 6; }
+  const int lane = e & 31, wid = e >> 5;  // wid: 0..31
+  if (opB == OP_N) { n = (wid & 7) * 8 + (lane >> 2); k = (wid >> 3) * 4 + (lane & 3); }
+  else { n = (wid & 7) * 8 + (lane & 7); k = (wid >> 3) * 4 + (lane >> 3); }
 }
 
 template <bool INLINE>
