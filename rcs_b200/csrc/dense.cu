@@ -535,8 +535,10 @@ __global__ void zcopy_grouped_kernel(const __grid_constant__ CopyArgs a) {
     const CopyProblem& P = probs[lo];
     const long u = t - start[lo];
     const int i = (int)(u % P.rows), j = (int)(u / P.rows);
-    zd v = P.conjTrans ? zconj(P.src[(size_t)i * P.lds + j]) : P.src[(size_t)j * P.lds + i];
-    P.dst[(size_t)j * P.ldd + i] = zmul(P.scale, v);
+    zd v = zmk(0, 0);  // src == nullptr: zero fill
+    if (P.src) v = zmul(P.scale, P.conjTrans ? zconj(P.src[(size_t)i * P.lds + j]) : P.src[(size_t)j * P.lds + i]);
+    zd* d = P.dst + (size_t)j * P.ldd + i;
+    *d = P.accumulate ? zadd(*d, v) : v;
   }
 }
 

@@ -57,12 +57,13 @@ void gemm_profile_enable(bool on);
 void gemm_profile_read(double* ms, double* flops, long* launches);
 
 struct CopyProblem {
-  const zd* src;
+  const zd* src;     // nullptr: dst is zero-filled
   zd* dst;
   int rows, cols;  // of dst
   int lds, ldd;
   int conjTrans;   // dst = conj(src)^T when set
   zd scale;        // dst = scale * src
+  int accumulate;  // dst += scale * src when set
 };
 void zcopy_grouped(aifmm_ctx* ctx, const std::vector<CopyProblem>& probs);
 void zfill(aifmm_ctx* ctx, zd* p, size_t n, zd v);

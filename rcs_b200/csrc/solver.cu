@@ -576,13 +576,16 @@ DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int
 // pivots and spans are those of the full pass, the basis of the old span is
 // the identity instead of a Householder rotation of it, and maxPivot of an
 // empty partition 2 is the unit norm of the first old column.
-DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel) {
+DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel,
+                  bool* prefix) {
   PhaseTimer pt(*this, stats.t_rrqr);
   const int m = A.r, n = A.c;
   stats.nRRQR++;
+  if (prefix) *prefix = false;
   if (!(orthoPanel && prm.orthoShortcut && partition > 0 && partition <= m))
     return rrqrRun(ops.copy(A), partition, inputPivot, fillRank, -1, maxPivot);
   stats.nRRQRShort++;
+  if (prefix) *prefix = true;  // Q_trunc = [old basis | new columns]
   const int r = partition, nf = n - partition;
   DMat Q1;  // view of the old basis
   Q1.buf = A.buf;
@@ -607,51 +610,90 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
   return Qt;
 }
 
-void Solver::updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P) {  // T:3159-3188
+void Solver::resizeRows(const std::vector<DMat*>& blocks, int rows) {
+  std::vector<CopyProblem> cps;
+  std::vector<DMat> keep;  // the old blocks stay alive until the copy is enqueued
+  for (DMat* b : blocks) {
+    DMat nw = ops.alloc(rows, b->c);
+    const int kept = std::min(rows, b->r);
+    if (kept > 0 && b->c > 0) cps.push_back({b->p, nw.p, kept, b->c, b->ld(), nw.ld(), 0, ONE});
+    if (rows > kept && b->c > 0) cps.push_back({nullptr, nw.p + kept, rows - kept, b->c, 1, nw.ld(), 0, ONE});
+    keep.push_back(*b);
+    *b = nw;
+  }
+  zcopy_grouped(ctx, cps);
+}
+
+void Solver::resizeCols(const std::vector<DMat*>& blocks, int cols) {
+  std::vector<CopyProblem> cps;
+  std::vector<DMat> keep;
+  for (DMat* b : blocks) {
+    DMat nw = ops.alloc(b->r, cols);
+    const int kept = std::min(cols, b->c);
+    if (kept > 0 && b->r > 0) cps.push_back({b->p, nw.p, b->r, kept, b->ld(), nw.ld(), 0, ONE});
+    if (cols > kept && b->r > 0)
+      cps.push_back({nullptr, nw.p + (size_t)kept * nw.ld(), b->r, cols - kept, 1, nw.ld(), 0, ONE});
+    keep.push_back(*b);
+    *b = nw;
+  }
+  zcopy_grouped(ctx, cps);
+}
+
+void Solver::updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P, bool prefix) {  // T:3159-3188
   opprof::Scope prof_("upd_m2l_k", ctx->stream);
   DBox& B = tree[j][k];
+  std::vector<DMat*> blocks;
+  for (auto& kv : B.P2L) blocks.push_back(&B.P2L[kv.first]);
+  for (int kIL : B.IL)
+    if (kIL != b) blocks.push_back(&B.M2L[kIL]);
+  for (int kN : B.NB)
+    if (kN != k && tree[j][kN].Eliminated && B.Eliminated) blocks.push_back(&B.M2L[kN]);
+  if (B.Eliminated) blocks.push_back(&B.M2L[k]);
+  if (prefix) {  // nL2P^H L2P = [I; 0] (or its first rows): keep rows, pad with zeros
+    resizeRows(blocks, nL2P.c);
+    return;
+  }
   const DMat T = ops.mul(nL2P, OP_C, B.L2P, OP_N);
   GemmBatch g;
   std::vector<DMat> keep;  // old blocks stay alive until the batched GEMM that reads them is launched
-  auto upd = [&](DMat& old) {
-    keep.push_back(old);
-    DMat nw = ops.alloc(T.r, old.c);
-    if (T.c == 0) nw = ops.zeros(T.r, old.c);
-    else g.add(nw, T, OP_N, old, OP_N, ONE, ZERO);
-    old = nw;
-  };
-  for (auto& kv : B.P2L) upd(B.P2L[kv.first]);
-  for (int kIL : B.IL)
-    if (kIL != b) upd(B.M2L[kIL]);
-  for (int kN : B.NB)
-    if (kN != k && tree[j][kN].Eliminated && B.Eliminated) upd(B.M2L[kN]);
-  if (B.Eliminated) upd(B.M2L[k]);
+  for (DMat* old : blocks) {
+    keep.push_back(*old);
+    DMat nw = ops.alloc(T.r, old->c);
+    if (T.c == 0) nw = ops.zeros(T.r, old->c);
+    else g.add(nw, T, OP_N, *old, OP_N, ONE, ZERO);
+    *old = nw;
+  }
   g.flush(ctx);
 }
 
-void Solver::updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt) {  // T:3252-3288
+void Solver::updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt, bool prefix) {  // T:3252-3288
   opprof::Scope prof_("upd_m2l_b", ctx->stream);
   DBox& Bb = tree[j][b];
+  std::vector<DMat*> blocks;
+  for (auto& kv : Bb.P2L) blocks.push_back(&tree[j][kv.first].M2P[b]);
+  for (int kIL : Bb.IL)
+    if (kIL != k) blocks.push_back(&tree[j][kIL].M2L[b]);
+  for (int kN : Bb.NB)
+    if (kN != b && tree[j][kN].Eliminated && Bb.Eliminated) blocks.push_back(&tree[j][kN].M2L[b]);
+  if (Bb.Eliminated) blocks.push_back(&Bb.M2L[b]);
+  if (prefix) {  // P2M nP2Mt = [I | 0] (or its first columns): keep columns, pad with zeros
+    resizeCols(blocks, nP2Mt.c);
+    return;
+  }
   const DMat S = ops.mul(Bb.P2M, OP_N, nP2Mt, OP_N);
   GemmBatch g;
   std::vector<DMat> keep;
-  auto upd = [&](DMat& old) {
-    keep.push_back(old);
-    DMat nw = ops.alloc(old.r, S.c);
-    if (S.r == 0) nw = ops.zeros(old.r, S.c);
-    else g.add(nw, old, OP_N, S, OP_N, ONE, ZERO);
-    old = nw;
-  };
-  for (auto& kv : Bb.P2L) upd(tree[j][kv.first].M2P[b]);
-  for (int kIL : Bb.IL)
-    if (kIL != k) upd(tree[j][kIL].M2L[b]);
-  for (int kN : Bb.NB)
-    if (kN != b && tree[j][kN].Eliminated && Bb.Eliminated) upd(tree[j][kN].M2L[b]);
-  if (Bb.Eliminated) upd(Bb.M2L[b]);
+  for (DMat* old : blocks) {
+    keep.push_back(*old);
+    DMat nw = ops.alloc(old->r, S.c);
+    if (S.r == 0) nw = ops.zeros(old->r, S.c);
+    else g.add(nw, *old, OP_N, S, OP_N, ONE, ZERO);
+    *old = nw;
+  }
   g.flush(ctx);
 }
 
-void Solver::updateParentL2P(int j, int k, const DMat& nL2P) {  // T:3290-3314
+void Solver::updateParentL2P(int j, int k, const DMat& nL2P, bool prefix) {  // T:3290-3314
   opprof::Scope prof_("upd_parent_l2p", ctx->stream);
   const int kP = k / nChild, c_k = k % nChild;
   DMat& PL = tree[j - 1][kP].L2P;
@@ -661,12 +703,13 @@ void Solver::updateParentL2P(int j, int k, const DMat& nL2P) {  // T:3290-3314
     U[c] = ops.block(PL, ri, 0, tree[j][kP * nChild + c].NumLocals, PL.c);
     ri += tree[j][kP * nChild + c].NumLocals;
   }
-  U[c_k] = ops.mul(ops.mul(nL2P, OP_C, tree[j][k].L2P, OP_N), OP_N, U[c_k], OP_N);
+  if (prefix) resizeRows({&U[c_k]}, nL2P.c);
+  else U[c_k] = ops.mul(ops.mul(nL2P, OP_C, tree[j][k].L2P, OP_N), OP_N, U[c_k], OP_N);
   PL = ops.vcat(U);
   tree[j - 1][kP].l2pOrtho = false;
 }
 
-void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt) {  // T:3316-3340
+void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt, bool prefix) {  // T:3316-3340
   opprof::Scope prof_("upd_parent_p2m", ctx->stream);
   const int bP = b / nChild, c_b = b % nChild;
   DMat& PM = tree[j - 1][bP].P2M;
@@ -676,33 +719,49 @@ void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt) {  // T:3316-3340
     V[c] = ops.block(PM, 0, ci, PM.r, tree[j][bP * nChild + c].NumMultipoles);
     ci += tree[j][bP * nChild + c].NumMultipoles;
   }
-  V[c_b] = ops.mul(ops.mul(V[c_b], OP_N, tree[j][b].P2M, OP_N), OP_N, nP2Mt, OP_N);
+  if (prefix) resizeCols({&V[c_b]}, nP2Mt.c);
+  else V[c_b] = ops.mul(ops.mul(V[c_b], OP_N, tree[j][b].P2M, OP_N), OP_N, nP2Mt, OP_N);
   PM = ops.hcatv(V);
   tree[j - 1][bP].p2mOrtho = false;
 }
 
 void Solver::compressP2PRRQR(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& P2Pt,
-                             DMat& nL2P, DMat& nP2Mt, DMat& newM2L) {  // T:1573-1656
+                             DMat& nL2P, DMat& nP2Mt, DMat& newM2L, bool& prefixL, bool& prefixM) {  // T:1573-1656
   double mp1, mp2;
-  nL2P = rrqr(ops.hcat(oldL2P, P2Pt), oldL2P.c, tree[j][k].maxPivot_L2P, fillin_rankVec[j], mp1, tree[j][k].l2pOrtho);
+  nL2P = rrqr(ops.hcat(oldL2P, P2Pt), oldL2P.c, tree[j][k].maxPivot_L2P, fillin_rankVec[j], mp1, tree[j][k].l2pOrtho,
+              &prefixL);
   tree[j][k].maxPivot_L2P = std::max(tree[j][k].maxPivot_L2P, mp1);
-  const DMat Rk = ops.mul(nL2P, OP_C, oldL2P, OP_N);
   const DMat Rkp = ops.mul(nL2P, OP_C, P2Pt, OP_N);
   nP2Mt = rrqr(ops.hcat(ops.adj(oldP2M), ops.adj(Rkp)), oldP2M.r, tree[j][b].maxPivot_P2M, fillin_rankVec[j], mp2,
-               tree[j][b].p2mOrtho);
+               tree[j][b].p2mOrtho, &prefixM);
   tree[j][b].maxPivot_P2M = std::max(tree[j][b].maxPivot_P2M, mp2);
-  const DMat Rn = ops.mul(nP2Mt, OP_C, oldP2M, OP_C);
   const DMat Rnp = ops.mul(nP2Mt, OP_C, Rkp, OP_C);
+  newM2L = ops.adj(Rnp);
   DMat& M = tree[j][k].M2L[b];
-  if (M.size() > 0) {
-    newM2L = ops.adj(Rnp);
-    GemmBatch g;
-    const DMat RkM = ops.mul(Rk, OP_N, M, OP_N);
-    g.add(newM2L, RkM, OP_N, Rn, OP_C, ONE, ONE);
-    g.flush(ctx);
-  } else {
-    newM2L = ops.adj(Rnp);
+  if (M.size() == 0) return;
+  // newM2L += Rk M Rn^H with Rk = nL2P^H oldL2P, Rn = nP2Mt^H oldP2M^H; a
+  // prefix basis makes its factor the partial identity [I; 0]
+  if (prefixL && prefixM) {  // M lands in the top-left block
+    const int r = std::min(M.r, newM2L.r), c = std::min(M.c, newM2L.c);
+    zcopy_grouped(ctx, {{M.p, newM2L.p, r, c, M.ld(), newM2L.ld(), 0, ONE, 1}});
+    return;
   }
+  DMat RkM;
+  if (prefixL) {
+    RkM = M;
+    resizeRows({&RkM}, nL2P.c);
+  } else {
+    RkM = ops.mul(ops.mul(nL2P, OP_C, oldL2P, OP_N), OP_N, M, OP_N);
+  }
+  if (prefixM) {  // (Rk M) [I 0]: add Rk M into the leading columns
+    const int r = std::min(RkM.r, newM2L.r), c = std::min(RkM.c, newM2L.c);
+    zcopy_grouped(ctx, {{RkM.p, newM2L.p, r, c, RkM.ld(), newM2L.ld(), 0, ONE, 1}});
+    return;
+  }
+  GemmBatch g;
+  const DMat Rn = ops.mul(nP2Mt, OP_C, oldP2M, OP_C);
+  g.add(newM2L, RkM, OP_N, Rn, OP_C, ONE, ONE);
+  g.flush(ctx);
 }
 
 static void equalise(Ops& ops, const DMat& L2P, const DMat& P2Mt, DMat& L2Pm, DMat& P2Mtm) {
@@ -720,23 +779,24 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   PhaseTimer pt(*this, stats.t_compress);
   stats.nCompressP2P++;
   DMat nL2P_k, nP2Mt_b, M2L_k_b, nL2P_b, nP2Mt_k, M2L_b_k;
+  bool pkL, pbM, pbL, pkM;  // which new bases start with the old ones
   {
     DMat a = tree[j][k].L2P, bb = tree[j][b].P2M, c = tree[j][k].P2P[b];
-    compressP2PRRQR(j, k, b, a, bb, c, nL2P_k, nP2Mt_b, M2L_k_b);
+    compressP2PRRQR(j, k, b, a, bb, c, nL2P_k, nP2Mt_b, M2L_k_b, pkL, pbM);
   }
   {
     DMat a = tree[j][b].L2P, bb = tree[j][k].P2M, c = tree[j][b].P2P[k];
-    compressP2PRRQR(j, b, k, a, bb, c, nL2P_b, nP2Mt_k, M2L_b_k);
+    compressP2PRRQR(j, b, k, a, bb, c, nL2P_b, nP2Mt_k, M2L_b_k, pbL, pkM);
   }
   DMat kL, kM, bL, bM;
   equalise(ops, nL2P_k, nP2Mt_k, kL, kM);
   equalise(ops, nL2P_b, nP2Mt_b, bL, bM);
   tree[j][k].M2L[b] = ops.block(M2L_k_b, 0, 0, kL.c, bM.c);
-  updateOtherM2LsAtK(j, k, b, kL);
-  updateOtherM2LsAtB(j, k, b, bM);
+  updateOtherM2LsAtK(j, k, b, kL, pkL);
+  updateOtherM2LsAtB(j, k, b, bM, pbM);
   if (j > startLevel) {
-    updateParentL2P(j, k, kL);
-    updateParentP2M(j, b, bM);
+    updateParentL2P(j, k, kL, pkL);
+    updateParentP2M(j, b, bM, pbM);
   }
   tree[j][k].L2P = kL;
   tree[j][b].P2M = ops.adj(bM);
@@ -744,11 +804,11 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   tree[j][k].NumLocals = tree[j][k].L2P.c;
   tree[j][b].NumMultipoles = tree[j][b].P2M.r;
   tree[j][b].M2L[k] = ops.block(M2L_b_k, 0, 0, bL.c, kM.c);
-  updateOtherM2LsAtK(j, b, k, bL);
-  updateOtherM2LsAtB(j, b, k, kM);
+  updateOtherM2LsAtK(j, b, k, bL, pbL);
+  updateOtherM2LsAtB(j, b, k, kM, pkM);
   if (j > startLevel) {
-    updateParentL2P(j, b, bL);
-    updateParentP2M(j, k, kM);
+    updateParentL2P(j, b, bL, pbL);
+    updateParentP2M(j, k, kM, pkM);
   }
   tree[j][b].L2P = bL;
   tree[j][k].P2M = ops.adj(kM);
@@ -764,41 +824,56 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   DBox& Bk = tree[j][k];
   // compress_M2P_myRRQR(j, k, b)
   double mp;
-  DMat nL2P_k = rrqr(ops.hcat(Bk.L2P, Bk.M2P[b]), Bk.L2P.c, Bk.maxPivot_L2P, fillin_rankVec[j], mp, Bk.l2pOrtho);
+  bool pL = false, pM = false;  // the new bases start with the old ones
+  DMat nL2P_k =
+      rrqr(ops.hcat(Bk.L2P, Bk.M2P[b]), Bk.L2P.c, Bk.maxPivot_L2P, fillin_rankVec[j], mp, Bk.l2pOrtho, &pL);
   Bk.maxPivot_L2P = std::max(Bk.maxPivot_L2P, mp);
-  DMat M2L_k_b;
+  DMat M2L_k_b = ops.mul(nL2P_k, OP_C, Bk.M2P[b], OP_N);  // Rk'
   {
-    const DMat Rk = ops.mul(nL2P_k, OP_C, Bk.L2P, OP_N);
-    M2L_k_b = ops.mul(nL2P_k, OP_C, Bk.M2P[b], OP_N);  // Rk'
-    GemmBatch g;
-    g.add(M2L_k_b, Rk, OP_N, Bk.M2L[b], OP_N, ONE, ONE);
-    g.flush(ctx);
+    const DMat& M = Bk.M2L[b];
+    if (pL) {  // Rk = [I; 0]: M2L[b] adds into the leading rows
+      if (M.size() > 0)
+        zcopy_grouped(ctx, {{M.p, M2L_k_b.p, std::min(M.r, M2L_k_b.r), std::min(M.c, M2L_k_b.c), M.ld(),
+                             M2L_k_b.ld(), 0, ONE, 1}});
+    } else {
+      const DMat Rk = ops.mul(nL2P_k, OP_C, Bk.L2P, OP_N);
+      GemmBatch g;
+      g.add(M2L_k_b, Rk, OP_N, M, OP_N, ONE, ONE);
+      g.flush(ctx);
+    }
   }
   // compress_P2L_myRRQR(j, b, k): A_row = [P2M_k^H | P2L[b][k]^H]
   DBox& Bb = tree[j][b];
-  DMat nP2Mt_k =
-      rrqr(ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k])), Bk.P2M.r, Bk.maxPivot_P2M, fillin_rankVec[j], mp, Bk.p2mOrtho);
+  DMat nP2Mt_k = rrqr(ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k])), Bk.P2M.r, Bk.maxPivot_P2M, fillin_rankVec[j], mp,
+                      Bk.p2mOrtho, &pM);
   Bk.maxPivot_P2M = std::max(Bk.maxPivot_P2M, mp);
   DMat M2L_b_k;
   {
-    const DMat Rn = ops.mul(nP2Mt_k, OP_C, Bk.P2M, OP_C);
     const DMat Rnp = ops.mul(nP2Mt_k, OP_C, Bb.P2L[k], OP_C);
     M2L_b_k = ops.adj(Rnp);
-    GemmBatch g;
-    g.add(M2L_b_k, Bb.M2L[k], OP_N, Rn, OP_C, ONE, ONE);
-    g.flush(ctx);
+    const DMat& M = Bb.M2L[k];
+    if (pM) {  // Rn^H = [I 0]: M2L[k] adds into the leading columns
+      if (M.size() > 0)
+        zcopy_grouped(ctx, {{M.p, M2L_b_k.p, std::min(M.r, M2L_b_k.r), std::min(M.c, M2L_b_k.c), M.ld(),
+                             M2L_b_k.ld(), 0, ONE, 1}});
+    } else {
+      const DMat Rn = ops.mul(nP2Mt_k, OP_C, Bk.P2M, OP_C);
+      GemmBatch g;
+      g.add(M2L_b_k, M, OP_N, Rn, OP_C, ONE, ONE);
+      g.flush(ctx);
+    }
   }
   DMat kL, kM;
   equalise(ops, nL2P_k, nP2Mt_k, kL, kM);
   Bk.M2L[b] = ops.block(M2L_k_b, 0, 0, kL.c, M2L_k_b.c);
-  updateOtherM2LsAtK(j, k, b, kL);
-  if (j > startLevel) updateParentL2P(j, k, kL);
+  updateOtherM2LsAtK(j, k, b, kL, pL);
+  if (j > startLevel) updateParentL2P(j, k, kL, pL);
   Bk.L2P = kL;
   Bk.l2pOrtho = true;
   Bk.NumLocals = Bk.L2P.c;
   Bb.M2L[k] = ops.block(M2L_b_k, 0, 0, M2L_b_k.r, kM.c);
-  updateOtherM2LsAtB(j, b, k, kM);
-  if (j > startLevel) updateParentP2M(j, k, kM);
+  updateOtherM2LsAtB(j, b, k, kM, pM);
+  if (j > startLevel) updateParentP2M(j, k, kM, pM);
   Bk.P2M = ops.adj(kM);
   Bk.p2mOrtho = true;
   Bk.NumMultipoles = Bk.P2M.r;

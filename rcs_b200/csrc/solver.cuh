@@ -103,13 +103,21 @@ class Solver {
   void eliminateZ(int j, int k);
   void compressP2PTwoWays(int j, int k, int b);
   void compressP2PRRQR(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& P2Pt, DMat& nL2P,
-                       DMat& nP2Mt, DMat& newM2L);
+                       DMat& nP2Mt, DMat& newM2L, bool& prefixL, bool& prefixM);
   void compressM2PP2L(int j, int k, int b);
-  void updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P);
-  void updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt);
-  void updateParentL2P(int j, int k, const DMat& nL2P);
-  void updateParentP2M(int j, int b, const DMat& nP2Mt);
-  DMat rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel);
+  // prefix: the new basis starts with the old one (the RRQR kept an
+  // orthonormal old basis), so the basis change is a partial identity and
+  // the products below reduce to row / column selection with zero padding.
+  void updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P, bool prefix);
+  void updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt, bool prefix);
+  void updateParentL2P(int j, int k, const DMat& nL2P, bool prefix);
+  void updateParentP2M(int j, int b, const DMat& nP2Mt, bool prefix);
+  // old blocks -> rows x old.c (first rows kept, zero below) / old.r x cols
+  // (first columns kept, zero right); one grouped copy for all of them
+  void resizeRows(const std::vector<DMat*>& blocks, int rows);
+  void resizeCols(const std::vector<DMat*>& blocks, int cols);
+  DMat rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel,
+            bool* prefix = nullptr);
   DMat rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot);
   void assignLeafRhs(const DMat& rhs);
   void rhsEliminateX(int j, int k);
