@@ -21,37 +21,84 @@ __device__ __forceinline__ zd ldB(const GemmProblem& P, int k, int j) {
   return zconj(P.B[(size_t)k * P.ldb + j]);
 }
 
-// acc += op(A) op(B) over the 64x64 tile at (row0, col0); K staged through
-// double-buffered shared slices with register prefetch of the next slice.
-__device__ __forceinline__ void gemm_tile_accumulate(const GemmProblem& P, int row0, int col0, zd (&acc)[4][4],
-                                                     zd (&As)[2][GBK][GBM], zd (&Bs)[2][GBK][GBN]) {
-  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-  const int t = threadIdx.x;
-  const int ai = t & 63, ak = t >> 6;
-  const int bk = t & 7, bj = t >> 3;
-  zd ra0 = ldA(P, row0 + ai, ak), ra1 = ldA(P, row0 + ai, ak + 4);
-  zd rb0 = ldB(P, bk, col0 + bj), rb1 = ldB(P, bk, col0 + bj + 32);
-  int buf = 0;
-  for (int k0 = 0; k0 < P.k; k0 += GBK) {
-    As[buf][ak][ai] = ra0;
-    As[buf][ak + 4][ai] = ra1;
-    Bs[buf][bk][bj] = rb0;
-    Bs[buf][bk][bj + 32] = rb1;
-    __syncthreads();
-    const int kn = k0 + GBK;
-    if (kn < P.k) {
-      ra0 = ldA(P, row0 + ai, kn + ak);
-      ra1 = ldA(P, row0 + ai, kn + ak + 4);
-      rb0 = ldB(P, kn + bk, col0 + bj);
-      rb1 = ldB(P, kn + bk, col0 + bj + 32);
-    }
+// acc += op(A) op(B) over the 64x64 tile at (row0, col0).  K advances in
+// slices of 16 through a three-stage shared-memory ring filled with
+// cp.async (16-byte copies, zero-filled outside the matrix), so two slices
+// are in flight while one is consumed; conjugation of op = C is applied when
+// an element is read from shared memory.
+constexpr int PBK = 16, PSTAGES = 3;
+struct GemmSmem {
+  zd A[PSTAGES][PBK][GBM];
+  zd B[PSTAGES][PBK][GBN];
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+  const uint32_t s = (uint32_t)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(valid ? 16 : 0));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+// Issue the copies of K slice kt into ring stage st: 1024 A and 1024 B
+// elements, four of each per thread, consecutive threads along the operand's
+// contiguous dimension.
+__device__ __forceinline__ void gemm_load_slice(const GemmProblem& P, int row0, int col0, int kt, GemmSmem& S, int st) {
+  const int k0 = kt * PBK;
 #pragma unroll
-    for (int kk = 0; kk < GBK; ++kk) {
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    int i, k;
+    if (P.opA == OP_N) { i = e & 63; k = e >> 6; }
+    else { k = e & 15; i = e >> 4; }
+    const int gi = row0 + i, gk = k0 + k;
+    const bool ok = gi < P.m && gk < P.k;
+    const zd* src = ok ? (P.opA == OP_N ? P.A + (size_t)gk * P.lda + gi : P.A + (size_t)gi * P.lda + gk) : P.A;
+    cp_async16(&S.A[st][k][i], src, ok);
+  }
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    const int e = threadIdx.x + 256 * q;
+    int j, k;
+    if (P.opB == OP_N) { k = e & 15; j = e >> 4; }
+    else { j = e & 63; k = e >> 6; }
+    const int gj = col0 + j, gk = k0 + k;
+    const bool ok = gj < P.n && gk < P.k;
+    const zd* src = ok ? (P.opB == OP_N ? P.B + (size_t)gj * P.ldb + gk : P.B + (size_t)gk * P.ldb + gj) : P.B;
+    cp_async16(&S.B[st][k][j], src, ok);
+  }
+}
+
+__device__ __forceinline__ void gemm_tile_accumulate(const GemmProblem& P, int row0, int col0, zd (&acc)[4][4],
+                                                     GemmSmem& S) {
+  const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
+  const int nk = (P.k + PBK - 1) / PBK;
+  const double sa = (P.opA == OP_N) ? 1.0 : -1.0, sb = (P.opB == OP_N) ? 1.0 : -1.0;  // imaginary sign
+#pragma unroll
+  for (int s = 0; s < PSTAGES - 1; ++s) {
+    if (s < nk) gemm_load_slice(P, row0, col0, s, S, s);
+    cp_async_commit();
+  }
+  for (int kt = 0; kt < nk; ++kt) {
+    cp_async_wait<PSTAGES - 2>();  // slice kt has landed (this thread's copies)
+    __syncthreads();               // ... and everyone's; stage of kt-1 is free
+    const int nxt = kt + PSTAGES - 1;
+    if (nxt < nk) gemm_load_slice(P, row0, col0, nxt, S, nxt % PSTAGES);
+    cp_async_commit();
+    const int st = kt % PSTAGES;
+#pragma unroll
+    for (int kk = 0; kk < PBK; ++kk) {
       zd a[4], b[4];
 #pragma unroll
-      for (int i = 0; i < 4; ++i) a[i] = As[buf][kk][tx + 16 * i];
+      for (int i = 0; i < 4; ++i) {
+        a[i] = S.A[st][kk][tx + 16 * i];
+        a[i].y *= sa;
+      }
 #pragma unroll
-      for (int j = 0; j < 4; ++j) b[j] = Bs[buf][kk][ty + 16 * j];
+      for (int j = 0; j < 4; ++j) {
+        b[j] = S.B[st][kk][ty + 16 * j];
+        b[j].y *= sb;
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -62,15 +109,15 @@ __device__ __forceinline__ void gemm_tile_accumulate(const GemmProblem& P, int r
           acc[i][j].y = fma(a[i].y, b[j].x, acc[i][j].y);
         }
     }
-    buf ^= 1;
   }
-  __syncthreads();  // the next chained problem reuses the shared slices
+  cp_async_wait<0>();
+  __syncthreads();  // the next chained problem reuses the ring
 }
 
 template <bool INLINE>
 __global__ void __launch_bounds__(256, 2) zgemm_grouped_kernel(const __grid_constant__ GemmArgs a) {
-  __shared__ zd As[2][GBK][GBM];
-  __shared__ zd Bs[2][GBK][GBN];
+  extern __shared__ unsigned char gemm_raw[];
+  GemmSmem& S = *reinterpret_cast<GemmSmem*>(gemm_raw);
   const GemmGroup* G = INLINE ? a.ig : a.groups;
   const GemmProblem* probs = INLINE ? a.ip : a.probs;
   int lo = 0, hi = a.ngroups - 1;
@@ -88,7 +135,8 @@ __global__ void __launch_bounds__(256, 2) zgemm_grouped_kernel(const __grid_cons
   for (int i = 0; i < 4; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = zmk(0, 0);
-  for (int q = 0; q < g.nchain; ++q) gemm_tile_accumulate(probs[g.head + q], row0, col0, acc, As, Bs);
+  for (int q = 0; q < g.nchain; ++q)
+    if (probs[g.head + q].k > 0) gemm_tile_accumulate(probs[g.head + q], row0, col0, acc, S);
   const GemmProblem& P = probs[g.head];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
@@ -494,8 +542,17 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     if (inl) zgemm_tf32x3_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
     else zgemm_tf32x3_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
   } else {
-    if (inl) zgemm_grouped_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
-    else zgemm_grouped_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
+    static bool attr[256] = {};
+    AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
+    if (!attr[ctx->device]) {
+      AIFMM_CUDA(cudaFuncSetAttribute(zgemm_grouped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(GemmSmem)));
+      AIFMM_CUDA(cudaFuncSetAttribute(zgemm_grouped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)sizeof(GemmSmem)));
+      attr[ctx->device] = true;
+    }
+    if (inl) zgemm_grouped_kernel<true><<<(unsigned)tiles, 256, sizeof(GemmSmem), ctx->stream>>>(a);
+    else zgemm_grouped_kernel<false><<<(unsigned)tiles, 256, sizeof(GemmSmem), ctx->stream>>>(a);
   }
   AIFMM_LAUNCHED();
   if (g_prof.on) {
