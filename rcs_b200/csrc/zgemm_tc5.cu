@@ -138,7 +138,7 @@ __device__ __forceinline__ void c5_coordB(int opB, int e, int& n, int& k) {
 }
 
 template <bool INLINE>
-__global__ void __launch_bounds__(C5_THREADS, 1) zgemm_tc5_kernel(const __grid_constant__ GemmArgs a) {
+__global__ void __launch_bounds__(C5_THREADS, 2) zgemm_tc5_kernel(const __grid_constant__ GemmArgs a) {
   extern __shared__ unsigned char c5_raw[];
   C5Smem& S = *reinterpret_cast<C5Smem*>((reinterpret_cast<uintptr_t>(c5_raw) + 1023) & ~uintptr_t(1023));
   const GemmGroup* G = INLINE ? a.ig : a.groups;
