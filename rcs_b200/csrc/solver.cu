@@ -907,12 +907,22 @@ void Solver::eliminateX(int j, int k) {
       coff.push_back(tot);
       tot += X.c;
     }
+    parts.push_back(ops.ident(m, ONE));  // the same solve yields P2P[k]^{-1} for the sweeps
+    const int invOff = tot;
     DMat W;
     {
       PhaseTimer t(*this, stats.t_msolve);
       W = ops.solve(B.luP2P, ops.hcatv(parts));
     }
     stats.flops_factor += 4.0 * m * (double)m * tot;
+    {
+      DMat inv;  // column range of W (ld = m), copied out so that W can go
+      inv.buf = W.buf;
+      inv.p = W.p + (size_t)invOff * W.ld();
+      inv.r = inv.c = m;
+      B.invP2P = ops.copy(inv);
+    }
+    B.luP2P = DLU();
     auto Wb = [&](int idx, int cols) {  // column slice view of W
       DMat v;
       v.buf = W.buf;
@@ -1042,8 +1052,10 @@ void Solver::eliminateZ(int j, int k) {
       v.c = cols;
       return v;
     };
-    const DMat Xy = Wb(0, B.NumMultipoles);
+    const DMat Xy = Wb(0, B.NumMultipoles);  // -L2M_f^{-1}
     B.M2L[k] = ops.copy(Xy);
+    B.negInvL2M = ops.copy(Xy);  // kept for the sweeps (M2L[k] is updated in place later)
+    B.luL2M = DLU();
     std::vector<DMat> T(nbs.size());
     for (size_t q = 0; q < nbs.size(); ++q) {
       const int nn = nbs[q];
@@ -1219,7 +1231,7 @@ void Solver::assignLeafRhs(const DMat& rhs) {  // T:670-678 (a gather of rows)
 void Solver::rhsEliminateX(int j, int k) {  // T:3613-3653, :3795-3886
   DBox& B = tree[j][k];
   if (B.P2P[k].size() != 0) {
-    const DMat y = ops.solve(B.luP2P, B.particle_rhs);
+    const DMat y = ops.mul(B.invP2P, OP_N, B.particle_rhs, OP_N);
     B.local_rhs = ops.mul(B.P2M, OP_N, y, OP_N, MONE);
     GemmBatch g;
     for (int nn : B.NB) {
@@ -1237,7 +1249,7 @@ void Solver::rhsEliminateX(int j, int k) {  // T:3613-3653, :3795-3886
 void Solver::rhsEliminateZ(int j, int k) {  // T:4115-4148, :4313-4397
   DBox& B = tree[j][k];
   if (B.L2M_f.size() > 0) {
-    B.multipole_rhs = ops.solve(B.luL2M, B.local_rhs);
+    B.multipole_rhs = ops.mul(B.negInvL2M, OP_N, B.local_rhs, OP_N, MONE);
     GemmBatch g;
     for (int nn : B.NB) {
       if (nn == k) continue;
@@ -1301,17 +1313,17 @@ void Solver::backSubstitute() {  // back_substitution_phase, T:4812-4865
         g.flush(ctx);
         // rhs2 = multipoles - P2M P2P_kk^{-1} rhs1 ; Atemp = -P2M P2P_kk^{-1} L2P = L2M_f
         DMat rhs2 = ops.copy(B.multipoles);
-        const DMat y = ops.solve(B.luP2P, rhs1);
+        const DMat y = ops.mul(B.invP2P, OP_N, rhs1, OP_N);
         GemmBatch g2;
         if (B.P2M.c > 0) g2.add(rhs2, B.P2M, OP_N, y, OP_N, MONE, ONE);
         g2.flush(ctx);
-        if (B.L2M_f.size() != 0) B.locals = ops.solve(B.luL2M, rhs2);
+        if (B.L2M_f.size() != 0) B.locals = ops.mul(B.negInvL2M, OP_N, rhs2, OP_N, MONE);
         else B.locals = ops.alloc(0, nrhs_);
         DMat t = rhs1;
         GemmBatch g3;
         if (B.L2P.c > 0) g3.add(t, B.L2P, OP_N, B.locals, OP_N, MONE, ONE);
         g3.flush(ctx);
-        B.particles = ops.solve(B.luP2P, t);
+        B.particles = ops.mul(B.invP2P, OP_N, t, OP_N);
       } else {
         B.particles = ops.alloc(0, nrhs_);
       }
@@ -1387,6 +1399,7 @@ std::vector<std::vector<DBox>> Solver::deepCopy(std::vector<std::vector<DBox>>& 
       dup(B.P2M);
       B.luP2P = DLU();
       B.luL2M = DLU();
+      B.invP2P = B.negInvL2M = DMat();
       B.hasLuP2P = B.hasLuL2M = false;
       B.particles = B.multipoles = B.locals = B.particle_rhs = B.multipole_rhs = B.local_rhs = DMat();
     }

@@ -45,7 +45,10 @@ struct DBox {
   DMat L2M_f, L2P, P2M;
   std::vector<int> chargeLocations, in_charge, in_check, out_charge, out_check;
   DMat Ac, Ar;
-  DLU luP2P, luL2M;  // stored factors of P2P[k] and L2M_f (the reference recomputes them in the sweeps)
+  DLU luP2P, luL2M;  // factors of P2P[k] and L2M_f, alive during the box's elimination
+  // P2P[k]^{-1} and -L2M_f^{-1}, kept for the solve sweeps (the reference
+  // refactorizes the blocks there); applied as multi-SM products
+  DMat invP2P, negInvL2M;
   // L2P has orthonormal columns / P2M orthonormal rows because a recompression
   // of this box produced them (not the ACA interpolation, not a parent update)
   bool l2pOrtho = false, p2mOrtho = false;
