@@ -3,13 +3,16 @@
     python -m rcs_b200.solver_bench [--sub 4] [--radius 0.15] [--freq 2e9] [--leaf 32]
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
                                     [--precision 0|1|2] [--op-tol 10] [--nrhs 8]
-                                    [--gmres 1e-6]
+                                    [--gmres 1e-6] [--profile-ops]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
 AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
 times one factorization and one solve (direct, or FGMRES to the target) and
 prints one JSON line with the solver's phase timers.  A small, single-pass
 workload for profiling the whole path (for example under a kernel profiler).
+--profile-ops repeats the factorization and the solve with the library's
+per-operation accounting on (every accounted operation then synchronises) and
+prints its table.
 """
 from __future__ import annotations
 
@@ -33,6 +36,7 @@ def main():
     ap.add_argument("--op-tol", type=int, default=10)
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--gmres", type=float, default=None)
+    ap.add_argument("--profile-ops", action="store_true")
     a = ap.parse_args()
     from . import mesh as M
     from .kernel import EFIEMatrix
@@ -45,6 +49,8 @@ def main():
     S = AIFMM(K, leaf_size=a.leaf, tol_pow=a.tol_pow, fillin_tol=a.fillin_tol, n_levels=a.levels,
               precision=a.precision)
     t_asm = time.perf_counter() - t0
+    if a.profile_ops:
+        S.checkpoint()
     A = H2Operator(K, leaf_size=a.leaf, tol_pow=a.op_tol, n_levels=a.levels) if a.gmres else None
     t0 = time.perf_counter()
     S.factorize()
@@ -57,6 +63,20 @@ def main():
         X = S.solve(B)
     t_sol = time.perf_counter() - t0
     info = S.info()
+    if a.profile_ops:
+        from .solver import profile_ops, profile_ops_read
+        S.rewind()
+        for what, fn in (("factorize", S.factorize), ("solve", lambda: S.solve(B))):
+            profile_ops(True)
+            t0 = time.perf_counter()
+            fn()
+            dt = time.perf_counter() - t0
+            rows = [ln.split() for ln in profile_ops_read().strip().splitlines()]
+            profile_ops(False)
+            print(f"# {what}: {dt:.3f} s with per-operation synchronisation")
+            print("| operation | calls | s |\n|---|---|---|")
+            for r in sorted(rows, key=lambda r: -float(r[2])):
+                print(f"| {r[0]} | {r[1]} | {float(r[2]):.3f} |")
     print(json.dumps({"N": K.N, "precision": a.precision, "assemble_s": t_asm, "factor_s": t_fac, "solve_s": t_sol,
                       "gmres": rec, "phases_s": {k: v for k, v in info.items() if k.startswith("t_")},
                       "rrqr": info["n_rrqr"], "flops_factor": info["flops_factor"]}), flush=True)
