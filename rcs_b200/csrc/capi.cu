@@ -123,7 +123,7 @@ int aifmm_profile_ops_read(char* buf, int cap) {
 int aifmm_tc5_timeouts(long* n) {
   API_BEGIN
   AIFMM_REQUIRE(n, AIFMM_EINVAL, "NULL argument");
-  *n = zgemm_tc5_timeouts();
+  *n = zgemm_tc5_timeouts() + zgemm_tc5p_timeouts();
   API_END
 }
 

@@ -482,7 +482,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
   long tiles = 0;
   double flops = 0;
   const int mode = ctx->gemmPrecision;
-  const int bm = (mode == 2) ? 128 : GBM;  // row tile of the tcgen05 kernel
+  const int bm = (mode >= 2) ? 128 : GBM;  // row tile of the tcgen05 kernels
   for (size_t i = 0; i < probs.size();) {
     const int len = chain[i];
     AIFMM_REQUIRE(len >= 1 && i + len <= probs.size(), AIFMM_EINVAL, "bad chain length");
@@ -536,7 +536,9 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     AIFMM_CUDA(cudaEventCreate(&e1));
     AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
   }
-  if (mode == 2) {
+  if (mode == 3) {
+    zgemm_tc5p(ctx, ps, gs, tiles);
+  } else if (mode == 2) {
     zgemm_tc5_launch(ctx, a, inl, tiles);
   } else if (mode == 1) {
     if (inl) zgemm_tf32x3_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);

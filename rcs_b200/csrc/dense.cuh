@@ -19,6 +19,10 @@ struct GemmProblem {
   int lda, ldb, ldc;
   int opA, opB;
   zd alpha, beta;
+  // split-TF32 planes of op(A) / op(B) in the tcgen05 tile layout (set by
+  // the launcher of the pre-tiled tensor-core GEMM; unused elsewhere)
+  const uint32_t* pa = nullptr;
+  const uint32_t* pb = nullptr;
 };
 
 // A group = a chain of problems accumulated into one C (consecutive in the
@@ -39,10 +43,16 @@ struct GemmArgs {
 };
 // Tensor-core (tcgen05) form of the split-TF32 grouped GEMM, 128x64 complex
 // tiles (zgemm_tc5.cu); groups must be tiled with tilesN = ceil(n / 64) and
-// ceil(m / 128) row tiles.  Returns false when the GPU cannot run it.
+// ceil(m / 128) row tiles.
 void zgemm_tc5_launch(aifmm_ctx* ctx, const GemmArgs& a, bool inl, long tiles);
 // Number of tcgen05 pipeline waits that ran out (each leaves its tile unwritten).
 long zgemm_tc5_timeouts();
+// The tensor-core GEMM over pre-tiled operand planes (zgemm_tc5p.cu): the
+// operands of every problem are first converted once into split-TF32 planes
+// laid out tile by tile, then each CTA streams its tiles with bulk copies.
+// Same tiling as zgemm_tc5_launch.
+long zgemm_tc5p_timeouts();
+void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<GemmGroup>& gs, long tiles);
 
 // C = alpha op(A) op(B) + beta C for every problem, one launch; the
 // problems must write disjoint C.

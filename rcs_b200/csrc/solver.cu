@@ -907,21 +907,21 @@ void Solver::eliminateX(int j, int k) {
       coff.push_back(tot);
       tot += X.c;
     }
-    parts.push_back(ops.ident(m, ONE));  // the same solve yields P2P[k]^{-1} for the sweeps
-    const int invOff = tot;
+    // W = P2P[k]^{-1} [L2P | X...]: the inverse from the LU (m columns), then
+    // one GEMM over all the neighbour columns instead of a triangular solve
+    // with thousands of right-hand sides; the inverse also serves the sweeps.
     DMat W;
     {
       PhaseTimer t(*this, stats.t_msolve);
-      W = ops.solve(B.luP2P, ops.hcatv(parts));
+      B.invP2P = ops.solve(B.luP2P, ops.ident(m, ONE));
+      const DMat X = ops.hcatv(parts);  // alive until the product is enqueued
+      W = ops.alloc(m, tot);
+      GemmBatch gw;
+      gw.add(W, B.invP2P, OP_N, X, OP_N, ONE, ZERO);
+      GemmPrecisionScope gp(ctx, prm.precision);  // the mixed path's tensor-core products
+      gw.flush(ctx);
     }
-    stats.flops_factor += 4.0 * m * (double)m * tot;
-    {
-      DMat inv;  // column range of W (ld = m), copied out so that W can go
-      inv.buf = W.buf;
-      inv.p = W.p + (size_t)invOff * W.ld();
-      inv.r = inv.c = m;
-      B.invP2P = ops.copy(inv);
-    }
+    stats.flops_factor += 4.0 * m * (double)m * m + 8.0 * m * (double)m * tot;
     B.luP2P = DLU();
     auto Wb = [&](int idx, int cols) {  // column slice view of W
       DMat v;

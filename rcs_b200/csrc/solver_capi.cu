@@ -13,7 +13,8 @@ extern "C" {
 int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out) {
   API_BEGIN
   AIFMM_REQUIRE(k && p && out, AIFMM_EINVAL, "NULL argument");
-  AIFMM_REQUIRE(p->precision >= 0 && p->precision <= 2, AIFMM_EINVAL, "precision must be 0 (plain), 1 or 2 (mixed)");
+  AIFMM_REQUIRE(p->precision >= 0 && p->precision <= 3, AIFMM_EINVAL,
+                "precision must be 0 (plain), 1, 2 or 3 (mixed)");
   AIFMM_REQUIRE(p->leaf_size > 0 && p->tol_pow >= 0 && p->fillin_tol >= 0 && p->n_levels >= 0, AIFMM_EINVAL,
                 "bad solver parameters");
   SolverParams sp;

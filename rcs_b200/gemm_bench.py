@@ -6,7 +6,9 @@
 Times C = A B (complex128 storage) through aifmm_zgemm_device with CUDA events
 on the library's stream, after warm-up, and prints one JSON line per
 precision: 0 = FP64 FMA (zgemm_grouped_kernel), 1 = split TF32 on the tensor
-cores by mma.sync, 2 = split TF32 by tcgen05 with tensor-memory accumulators.
+cores by mma.sync, 2 = split TF32 by tcgen05 with tensor-memory accumulators
+and the split inside the tile loop, 3 = the same with the operands split once
+into pre-tiled planes that the tile loop streams with bulk copies.
 Flops are complex-counted (8 m n k per product).  --batch B issues B
 independent products per launch (the grouped form the solver uses).  The
 operands total more than the 126 MB L2 for the default size with --batch 8.
@@ -64,7 +66,7 @@ def main():
     ap.add_argument("--m", type=int, default=2048)
     ap.add_argument("--n", type=int, default=2048)
     ap.add_argument("--k", type=int, default=2048)
-    ap.add_argument("--precision", type=int, nargs="+", default=[0, 1, 2])
+    ap.add_argument("--precision", type=int, nargs="+", default=[0, 1, 2, 3])
     ap.add_argument("--reps", type=int, default=20)
     ap.add_argument("--batch", type=int, default=1)
     a = ap.parse_args()

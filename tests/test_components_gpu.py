@@ -107,7 +107,7 @@ def test_lu_solve(nrhs):
         assert np.linalg.norm(A @ X - B) / np.linalg.norm(B) < 1e-10
 
 
-@pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6), (2, 2e-6)])
+@pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6), (2, 2e-6), (3, 2e-6)])
 @pytest.mark.parametrize("m,n,k,opA,opB", [
     (64, 64, 16, 0, 0), (1, 1, 1, 0, 0), (65, 33, 17, 1, 0), (200, 130, 451, 0, 1), (37, 300, 5, 1, 1),
     (10, 10, 0, 0, 0),
@@ -123,7 +123,7 @@ def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
     ref = alpha * ((A.conj().T if opA else A) @ (B.conj().T if opB else B)) + beta * C0
     scale = abs(alpha) * np.linalg.norm(A) * np.linalg.norm(B) + abs(beta) * np.linalg.norm(C0)
     assert np.linalg.norm(C - ref) <= bound * scale
-    if precision == 2:  # no tcgen05 pipeline wait ran out
+    if precision >= 2:  # no tcgen05 pipeline wait ran out
         import ctypes as Cc
         from rcs_b200 import _lib
         n_to = Cc.c_long()

@@ -121,10 +121,10 @@ def test_mixed_precision_factorization_refines_to_target():
     b = K.planeWaveRhs((0, 0, -1), (1, 0, 0))
     A = H2Operator(K, leaf_size=16, tol_pow=11, n_levels=3)
     res = {}
-    for prec in (0, 1):
+    for prec in (0, 1, 3):
         S = AIFMM(K, leaf_size=16, tol_pow=6, fillin_tol=8, n_levels=3, precision=prec)
         S.factorize()
         res[prec] = np.linalg.norm(Z @ S.solve(b) - b) / np.linalg.norm(b)
         x, rec = S.solve_gmres(A, b, tol=1e-8)
         assert np.linalg.norm(Z @ x - b) / np.linalg.norm(b) < 2e-8, (prec, rec)
-    assert res[1] < max(10 * res[0], 1e-5), res
+    assert res[1] < max(10 * res[0], 1e-5) and res[3] < max(10 * res[0], 1e-5), res
