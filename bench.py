@@ -40,12 +40,12 @@ CONFIGS = {
                desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10, "
                     "direct solve"),
     "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
-               gmres=1e-6, precision=2,
+               gmres=1e-6, precision=3,
                desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
-                    "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs) as the "
-                    "preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
+                    "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs over pre-tiled "
+                    "planes) as the preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
     "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
-                gmres=1e-6, precision=2,
+                gmres=1e-6, precision=3,
                 desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
                      "8 plane waves, FGMRES(30) to 1e-6 (c3 shape at 1/4 size)"),
 }
@@ -411,7 +411,9 @@ def main():
             "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs,
                        "path": ({0: "plain complex128 factorization (reference control flow)",
                                  1: "mixed factorization (split-TF32 mma.sync GEMMs)",
-                                 2: "mixed factorization (split-TF32 tcgen05 GEMMs)"}[cfg.get("precision", 0)]
+                                 2: "mixed factorization (split-TF32 tcgen05 GEMMs)",
+                                 3: "mixed factorization (split-TF32 tcgen05 GEMMs, pre-tiled planes)"}
+                                [cfg.get("precision", 0)]
                                 + (" + FP64 FGMRES" if A is not None else ", direct solve")),
                        "parallelism": "replicas" if world > 1 else "single GPU",
                        "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"},
@@ -424,7 +426,9 @@ def main():
             "tree": {"levels": info["n_levels"], "avg_leaf": info["avg_leaf_size"], "avg_rank": info["avg_multipoles"],
                      "max_rank": info["max_rank"], "rrqr": info["n_rrqr"]},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "zgemm_grouped_kernel", "achieved": achieved,
+            "roofline": {"bound": "tensor", "kernel": "grouped GEMM launches of the step (FP64 zgemm_grouped_kernel "
+                                                "and, on the mixed path, the tcgen05 Schur products)",
+                         "achieved": achieved,
                          "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
                          "peak_source": "measured cuBLAS complex128 GEMM 4096^3 on this GPU (FP64 path; "
                                         "MEASURED_PEAKS.json has no FP64 figure)",

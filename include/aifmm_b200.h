@@ -134,7 +134,8 @@ int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int to
  * op: 0 none, 1 conjugate transpose) through the solver's grouped GEMM:
  * precision 0 = FP64 FMA; 1 and 2 = split-TF32 tensor cores with FP32
  * accumulation (FP32 accuracy): 1 by warp-level mma.sync, 2 by tcgen05 with
- * tensor-memory accumulators.  The dense products of the reference go through Eigen;
+ * tensor-memory accumulators, 3 by tcgen05 over operands split once into
+ * pre-tiled planes streamed with bulk copies.  The dense products of the reference go through Eigen;
  * this is the kernel that replaces them on the GPU. */
 int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
@@ -159,7 +160,9 @@ typedef struct {
                     * 1e-5 relative at K = 2048) while the box LU factors, RRQR,
                     * pivots, norms and solves stay FP64 -- a preconditioner for
                     * aifmm_solver_solve_gmres; 2 = the same with the tcgen05
-                    * kernel (tensor-memory accumulators) instead of mma.sync */
+                    * kernel (tensor-memory accumulators) instead of mma.sync;
+                    * 3 = tcgen05 over operands split once into pre-tiled planes
+                    * (the fastest form) */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
                     * Householder pass, as the reference does; 0 (default) skips
                     * that pass when the old basis is one this solver produced with
