@@ -18,6 +18,7 @@
 // alpha, beta in FP64.  Every wait is bounded (one second); a wait that runs
 // out leaves the tile unwritten and is counted (zgemm_tc5p_timeouts()).
 #include <algorithm>
+#include <map>
 
 #include "dense.cuh"
 
@@ -314,37 +315,72 @@ __global__ void __launch_bounds__(P5_THREADS, 1) zgemm_tc5p_kernel(const __grid_
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P5_TMEM_COLS) : "memory");
 }
 
-void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<GemmGroup>& gs, long tiles) {
-  // plane buffers of every problem, one allocation
-  std::vector<P5Operand> ops;
-  std::vector<long> start;
+namespace {
+// An operand as the conversion sees it; problems that read the same matrix
+// the same way share its planes.
+struct P5Key {
+  const zd* src;
+  int ld, op, rows, k, isB;
+  bool operator<(const P5Key& o) const {
+    if (src != o.src) return src < o.src;
+    if (ld != o.ld) return ld < o.ld;
+    if (op != o.op) return op < o.op;
+    if (rows != o.rows) return rows < o.rows;
+    if (k != o.k) return k < o.k;
+    return isB < o.isB;
+  }
+};
+size_t p5_words(const P5Key& key) {
+  const int tr = key.isB ? P5_N : P5_M;
+  const int nks = std::max(1, (key.k + P5_KS - 1) / P5_KS);
+  return (size_t)((key.rows + tr - 1) / tr) * nks * (key.isB ? P5_B_BYTES : P5_A_BYTES) / 4;
+}
+constexpr size_t P5_PLANE_BUDGET = (size_t)4 << 30;  // bytes of planes per launch
+}  // namespace
+
+// Converts the distinct operands of a run of groups and launches their tiles.
+static void p5_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const std::vector<GemmGroup>& gs, size_t g0,
+                      size_t g1) {
+  std::map<P5Key, size_t> where;  // operand -> word offset of its planes
   size_t words = 0;
-  std::vector<std::pair<size_t, size_t>> off(ps.size());
-  for (size_t i = 0; i < ps.size(); ++i) {
-    const GemmProblem& p = ps[i];
-    const int nks = std::max(1, (p.k + P5_KS - 1) / P5_KS);
-    const size_t wa = (size_t)((p.m + P5_M - 1) / P5_M) * nks * (P5_A_BYTES / 4);
-    const size_t wb = (size_t)((p.n + P5_N - 1) / P5_N) * nks * (P5_B_BYTES / 4);
-    off[i] = {words, words + wa};
-    words += wa + wb;
+  std::vector<GemmProblem> ps;
+  std::vector<GemmGroup> groups;
+  long tiles = 0;
+  for (size_t gi = g0; gi < g1; ++gi) {
+    GemmGroup g = gs[gi];
+    const int head = (int)ps.size();
+    for (int q = 0; q < g.nchain; ++q) {
+      GemmProblem p = all[g.head + q];
+      const P5Key ka{p.A, p.lda, p.opA, p.m, p.k, 0}, kb{p.B, p.ldb, p.opB, p.n, p.k, 1};
+      for (const P5Key& key : {ka, kb})
+        if (!where.count(key)) {
+          where[key] = words;
+          words += p5_words(key);
+        }
+      ps.push_back(p);
+    }
+    const int nrt = (all[g.head].m + P5_M - 1) / P5_M;
+    g.head = head;
+    g.tileStart = (int)tiles;
+    tiles += (long)nrt * g.tilesN;
+    groups.push_back(g);
   }
   DevBuf planes(ctx, sizeof(uint32_t) * std::max<size_t>(words, 4));
   uint32_t* base = planes.as<uint32_t>();
+  std::vector<P5Operand> ops;
+  std::vector<long> start;
   long total = 0;
-  for (size_t i = 0; i < ps.size(); ++i) {
-    GemmProblem& p = ps[i];
-    p.pa = base + off[i].first;
-    p.pb = base + off[i].second;
-    if (p.k <= 0) continue;
-    const int nks = (p.k + P5_KS - 1) / P5_KS;
-    const P5Operand oa{p.A, base + off[i].first, p.m, p.k, p.lda, p.opA, 0, nks};
-    const P5Operand ob{p.B, base + off[i].second, p.n, p.k, p.ldb, p.opB, 1, nks};
-    for (const P5Operand& o : {oa, ob}) {
-      const int tr = o.isB ? P5_N : P5_M;
-      ops.push_back(o);
-      start.push_back(total);
-      total += (long)((o.rows + tr - 1) / tr) * tr * (o.nks * P5_KS);
-    }
+  for (const auto& kv : where) {
+    const P5Key& key = kv.first;
+    if (key.k <= 0) continue;
+    const int nks = (key.k + P5_KS - 1) / P5_KS, tr = key.isB ? P5_N : P5_M;
+    ops.push_back({key.src, base + kv.second, key.rows, key.k, key.ld, key.op, key.isB, nks});
+    start.push_back(total);
+    total += (long)((key.rows + tr - 1) / tr) * tr * (nks * P5_KS);
+  }
+  for (GemmProblem& p : ps) {
+    p.pa = base + where[P5Key{p.A, p.lda, p.opA, p.m, p.k, 0}];
+    p.pb = base + where[P5Key{p.B, p.ldb, p.opB, p.n, p.k, 1}];
   }
   if (total > 0) {
     DevBuf dops = upload(ctx, ops), dst = upload(ctx, start);
@@ -352,18 +388,20 @@ void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<G
     p5_convert_kernel<<<grid, 256, 0, ctx->stream>>>(dops.as<P5Operand>(), dst.as<long>(), (int)ops.size(), total);
     AIFMM_LAUNCHED();
   }
+  if (tiles <= 0) return;
+  AIFMM_REQUIRE(tiles < (long)INT32_MAX, AIFMM_EOVERFLOW, "too many GEMM tiles");
   GemmArgs a;
-  a.ngroups = (int)gs.size();
+  a.ngroups = (int)groups.size();
   a.probs = nullptr;
   a.groups = nullptr;
   DevBuf dp, dg;
-  const bool inl = gs.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
+  const bool inl = groups.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
   if (inl) {
     std::copy(ps.begin(), ps.end(), a.ip);
-    std::copy(gs.begin(), gs.end(), a.ig);
+    std::copy(groups.begin(), groups.end(), a.ig);
   } else {
     dp = upload(ctx, ps);
-    dg = upload(ctx, gs);
+    dg = upload(ctx, groups);
     a.probs = dp.as<GemmProblem>();
     a.groups = dg.as<GemmGroup>();
   }
@@ -378,6 +416,38 @@ void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<G
   if (inl) zgemm_tc5p_kernel<true><<<(unsigned)tiles, P5_THREADS, smem, ctx->stream>>>(a);
   else zgemm_tc5p_kernel<false><<<(unsigned)tiles, P5_THREADS, smem, ctx->stream>>>(a);
   AIFMM_LAUNCHED();
+}
+
+// Groups are launched in runs whose distinct operands fit the plane budget
+// (a group larger than the budget runs alone).
+void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<GemmGroup>& gs, long) {
+  size_t g0 = 0;
+  while (g0 < gs.size()) {
+    std::map<P5Key, bool> seen;
+    size_t bytes = 0, g1 = g0;
+    while (g1 < gs.size()) {
+      size_t add = 0;
+      std::vector<P5Key> fresh;
+      for (int q = 0; q < gs[g1].nchain; ++q) {
+        const GemmProblem& p = ps[gs[g1].head + q];
+        for (const P5Key& key : {P5Key{p.A, p.lda, p.opA, p.m, p.k, 0}, P5Key{p.B, p.ldb, p.opB, p.n, p.k, 1}})
+          if (!seen.count(key)) {
+            bool dup = false;
+            for (const P5Key& f : fresh) dup = dup || !(f < key || key < f);
+            if (!dup) {
+              fresh.push_back(key);
+              add += 4 * p5_words(key);
+            }
+          }
+      }
+      if (g1 > g0 && bytes + add > P5_PLANE_BUDGET) break;
+      for (const P5Key& f : fresh) seen[f] = true;
+      bytes += add;
+      ++g1;
+    }
+    p5_launch(ctx, ps, gs, g0, g1);
+    g0 = g1;
+  }
 }
 
 long zgemm_tc5p_timeouts() {
