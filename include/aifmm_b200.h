@@ -99,6 +99,18 @@ int aifmm_kernel_rhs_plane(aifmm_kernel* k, const double khat[3], const double e
  * (ElectrostaticsMatrix::getRhs, :374-381). */
 int aifmm_kernel_rhs_conductor(aifmm_kernel* k, int conductor, double* out);
 
+/* Surface current at the triangle centroids of an EFIE solution, as
+ * EFIEMatrix::getJAtCentroids (src/EFIEMatrix.cpp:1100-1130): coeff holds the
+ * n RWG coefficients (complex), J receives n_tris x 3 complex values,
+ * column-major (the reference's MatrixXcd JAtCentroids). */
+int aifmm_kernel_currents(aifmm_kernel* k, const double* coeff, double* J);
+/* Bistatic radar cross-section of centroid currents J (n_tris x 3 complex,
+ * column-major) at n_angles observation directions (theta[a], phi[a]) by the
+ * one-point rule of EFIEMatrix::getRCS_OnePointQuadrature (:916-930), with the
+ * kernel's wavenumber; rcs receives n_angles values. */
+int aifmm_kernel_rcs(aifmm_kernel* k, const double* J, int n_angles, const double* theta, const double* phi,
+                     double* rcs);
+
 /* ---- low-rank and dense components ----------------------------------------- */
 /* Partially pivoted ACA of K(rows, cols): replaces
  * LowRank<K>::ACA_only_nodes2(row_bases, col_bases, rank, Ac, Ar)
@@ -114,6 +126,16 @@ int aifmm_aca(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc,
  * selects the real Householder sign of a USE_DOUBLE build. */
 int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
                double input_pivot, int fill_rank, int real_mode, double* Q, int* rank, double* max_pivot);
+/* The same RRQR with its other outputs, for RRQR::R_trunc and RRQR::P
+ * (include/rrqr.hpp:5-27): R (rank x n complex, leading dimension rank; a
+ * buffer of min(m, n) x n) receives R_trunc = Q_trunc^H A P, upper trapezoidal,
+ * and perm (n ints) the column order of A P: column q of A P is column perm[q]
+ * of A.  The first rank entries of perm are the reference's pivots; the order
+ * of the remaining columns differs, because the reference re-sorts them at
+ * every step while this kernel swaps the pivot into place. */
+int aifmm_rrqr_full(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
+                    double input_pivot, int fill_rank, int real_mode, double* Q, double* R, int* perm, int* rank,
+                    double* max_pivot);
 /* The same RRQR for callers that cannot allocate device memory (code running
  * inside another framework's allocator, during stream capture, or under a
  * pre-reserved memory budget).  No counterpart in the reference.  Every
@@ -193,6 +215,17 @@ typedef struct {
  * (getNodes), the L2P/P2M operators, the M2L blocks and the leaf P2P blocks,
  * all resident in device memory. */
 int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out);
+/* The same with the tree built over caller-given unknown locations (xyz,
+ * n x 3 row-major, n = the kernel's size) inside the box domain = {xmin, xmax,
+ * ymin, ymax, zmin, zmax} (NULL: the locations' bounding box), as
+ * inputsToSolverClass::locations and xmin..zmax (include/includes.hpp:73-77)
+ * feed FMM2DTree's constructor.  The box must contain every location. */
+int aifmm_solver_create_at(aifmm_kernel* k, const aifmm_solver_params* p, const double* xyz, int n,
+                           const double domain[6], aifmm_solver** out);
+/* The tree order of the unknowns: order[p] = the unknown at position p of the
+ * leaf-by-leaf vector that FMM2DTree::getx assembles before reorder
+ * (T:4874-4907, T:466-476 of the tree header). */
+int aifmm_solver_tree_order(aifmm_solver* s, int* order);
 /* AIFMM<K>::factorize() -> eliminate_phase_efficient (src/AIFMM.cpp:96-100). */
 int aifmm_solver_factorize(aifmm_solver* s);
 /* backSubstitute1/2/3 + getPhi (src/AIFMM.cpp:120-147) for nrhs right-hand

@@ -42,7 +42,11 @@ SIGNATURES = {
     "aifmm_kernel_rhs_reference": (_i, [_p, _dp, _dp]),
     "aifmm_kernel_rhs_plane": (_i, [_p, _dp, _dp, _dp]),
     "aifmm_kernel_rhs_conductor": (_i, [_p, _i, _dp]),
+    "aifmm_kernel_currents": (_i, [_p, _dp, _dp]),
+    "aifmm_kernel_rcs": (_i, [_p, _dp, _i, _dp, _dp, _dp]),
     "aifmm_solver_create": (_i, [_p, _p, _pp]),
+    "aifmm_solver_create_at": (_i, [_p, _p, _dp, _i, _p, _pp]),
+    "aifmm_solver_tree_order": (_i, [_p, _ip]),
     "aifmm_solver_factorize": (_i, [_p]),
     "aifmm_solver_solve": (_i, [_p, _dp, _i, _dp]),
     "aifmm_solver_solve_device": (_i, [_p, _p, _i, _p]),
@@ -56,6 +60,7 @@ SIGNATURES = {
     "aifmm_profile_ops_read": (_i, [C.c_char_p, _i]),
     "aifmm_aca": (_i, [_p, _ip, _i, _ip, _i, _d, _ip, _ip, C.POINTER(_i), _dp, _dp]),
     "aifmm_rrqr": (_i, [_p, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, C.POINTER(_i), C.POINTER(_d)]),
+    "aifmm_rrqr_full": (_i, [_p, _dp, _i, _i, _i, _i, _i, _d, _i, _i, _dp, _dp, _ip, C.POINTER(_i), C.POINTER(_d)]),
     "aifmm_rrqr_noalloc": (_i, [_p, _i, _i, _i, _i, _i, _d, _i, _i, _p, _p, _p, _p]),
     "aifmm_lu_solve": (_i, [_p, _dp, _i, _dp, _i, _dp]),
     "aifmm_zgemm": (_i, [_p, _i, _i, _i, _i, _i, _i, _dp, _dp, _i, _dp, _i, _dp, _dp, _i]),

@@ -68,9 +68,16 @@ int aifmm_aca(aifmm_kernel* k, const int* rows, int nr, const int* cols, int nc,
   API_END
 }
 
-int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
-               double input_pivot, int fill_rank, int real_mode, double* Q, int* rank, double* max_pivot) {
-  API_BEGIN
+static void zgemm_checked(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double* alpha,
+                          const zd* A, int lda, const zd* B, int ldb, const double* beta, zd* C, int ldc);
+
+// Host-array RRQR shared by aifmm_rrqr and aifmm_rrqr_full; R and perm may be
+// NULL.  R_trunc is formed as Q_trunc^H (A P), which equals the reference's
+// rows 0..rank-1 of the transformed matrix; the entries below the diagonal of
+// its leading rank x rank block are exact zeros there and are set so here.
+static void rrqr_host(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
+                      double input_pivot, int fill_rank, int real_mode, double* Q, double* Rt, int* perm_out,
+                      int* rank, double* max_pivot) {
   AIFMM_REQUIRE(ctx && A && Q && rank && max_pivot, AIFMM_EINVAL, "NULL argument");
   AIFMM_REQUIRE(m > 0 && n > 0 && partition >= 0 && partition <= n, AIFMM_EINVAL, "bad sizes");
   AIFMM_REQUIRE(tol_pow1 >= 0 && tol_pow2 >= 0 && fill_rank >= 0, AIFMM_EINVAL, "negative tolerance power or fill-in rank");
@@ -109,7 +116,42 @@ int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int
   *max_pivot = h.mp;
   if (h.r > 0)
     AIFMM_CUDA(cudaMemcpyAsync(Q, Qd.p, sizeof(zd) * (size_t)m * h.r, cudaMemcpyDeviceToHost, ctx->stream));
+  if (perm_out || Rt) {
+    std::vector<int> hp(n);
+    AIFMM_CUDA(cudaMemcpyAsync(hp.data(), perm.p, sizeof(int) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+    if (perm_out) std::memcpy(perm_out, hp.data(), sizeof(int) * n);
+    if (Rt && h.r > 0) {
+      const zd* Ah = reinterpret_cast<const zd*>(A);
+      std::vector<zd> ap((size_t)m * n);
+      for (int q = 0; q < n; ++q) std::memcpy(&ap[(size_t)q * m], Ah + (size_t)hp[q] * m, sizeof(zd) * m);
+      DevBuf APd = upload(ctx, ap), Rd(ctx, sizeof(zd) * (size_t)h.r * n);
+      const double one[2] = {1.0, 0.0}, zero[2] = {0.0, 0.0};
+      zgemm_checked(ctx, 0, 1, 0, h.r, n, m, one, Qd.as<zd>(), m, APd.as<zd>(), m, zero, Rd.as<zd>(), h.r);
+      AIFMM_CUDA(cudaMemcpyAsync(Rt, Rd.p, sizeof(zd) * (size_t)h.r * n, cudaMemcpyDeviceToHost, ctx->stream));
+      AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+      for (int q = 0; q < std::min(h.r, n); ++q)
+        for (int i = q + 1; i < h.r; ++i) Rt[2 * ((size_t)q * h.r + i)] = Rt[2 * ((size_t)q * h.r + i) + 1] = 0.0;
+    }
+  }
   AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+}
+
+int aifmm_rrqr(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
+               double input_pivot, int fill_rank, int real_mode, double* Q, int* rank, double* max_pivot) {
+  API_BEGIN
+  rrqr_host(ctx, A, m, n, partition, tol_pow1, tol_pow2, input_pivot, fill_rank, real_mode, Q, nullptr, nullptr,
+            rank, max_pivot);
+  API_END
+}
+
+int aifmm_rrqr_full(aifmm_ctx* ctx, const double* A, int m, int n, int partition, int tol_pow1, int tol_pow2,
+                    double input_pivot, int fill_rank, int real_mode, double* Q, double* R, int* perm, int* rank,
+                    double* max_pivot) {
+  API_BEGIN
+  AIFMM_REQUIRE(R && perm, AIFMM_EINVAL, "NULL argument");
+  rrqr_host(ctx, A, m, n, partition, tol_pow1, tol_pow2, input_pivot, fill_rank, real_mode, Q, R, perm, rank,
+            max_pivot);
   API_END
 }
 

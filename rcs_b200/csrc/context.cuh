@@ -83,6 +83,7 @@ struct aifmm_kernel {
   aifmm_ctx* ctx = nullptr;
   aifmm::KernelGeom geom;
   aifmm::DevBuf d_tri, d_node, d_rwg, d_len, d_side;
+  aifmm::DevBuf d_t2e_off, d_t2e_inc;  // EFIE: triangle -> RWG edge incidence, built on first use
   std::vector<double> locations;   // N x 3
   std::vector<int> cond;           // electrostatics: conductor per triangle
   std::vector<int> rwg_host;       // EFIE: N x 4

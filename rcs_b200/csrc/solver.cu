@@ -40,14 +40,22 @@ struct PhaseTimer {
 };
 
 // ------------------------------------------------------------ setup, T:52-165
-Solver::Solver(aifmm_kernel* k, const SolverParams& p) : K(k), ctx(k->ctx), ops(k->ctx), prm(p) {
+Solver::Solver(aifmm_kernel* k, const SolverParams& p, const double* xyz, const double* dom)
+    : K(k), ctx(k->ctx), ops(k->ctx), prm(p) {
   N = k->geom.N;
-  particles = k->locations;
+  particles = xyz ? std::vector<double>(xyz, xyz + 3 * (size_t)N) : k->locations;
   double mn[3] = {1e300, 1e300, 1e300}, mx[3] = {-1e300, -1e300, -1e300};
   for (int i = 0; i < N; ++i)
     for (int q = 0; q < 3; ++q) {
       mn[q] = std::min(mn[q], particles[3 * i + q]);
       mx[q] = std::max(mx[q], particles[3 * i + q]);
+    }
+  if (dom)
+    for (int q = 0; q < 3; ++q) {
+      AIFMM_REQUIRE(dom[2 * q] <= mn[q] && dom[2 * q + 1] >= mx[q], AIFMM_EINVAL,
+                    "the domain box does not contain every location");
+      mn[q] = dom[2 * q];
+      mx[q] = dom[2 * q + 1];
     }
   for (int q = 0; q < 3; ++q) {
     domain[2 * q] = mn[q];

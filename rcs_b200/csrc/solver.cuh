@@ -74,7 +74,10 @@ class Solver {
   double domain[6];
   bool factored = false;
 
-  Solver(aifmm_kernel* k, const SolverParams& p);
+  // xyz (N x 3) and dom (xmin, xmax, ymin, ymax, zmin, zmax) replace the
+  // kernel's unknown locations and their bounding box when given, as
+  // inputsToSolverClass::locations and xmin..zmax do in the reference.
+  Solver(aifmm_kernel* k, const SolverParams& p, const double* xyz = nullptr, const double* dom = nullptr);
   void build();
   void factorize();
   // rhs: N x nrhs (device), returns x: N x nrhs (device)

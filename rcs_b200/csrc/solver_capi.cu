@@ -1,4 +1,5 @@
 // C ABI of the AIFMM solver (see include/aifmm_b200.h).
+#include <cmath>
 #include <cstdlib>
 #include <memory>
 
@@ -10,8 +11,8 @@ using namespace aifmm;
 
 extern "C" {
 
-int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out) {
-  API_BEGIN
+static void solver_create(aifmm_kernel* k, const aifmm_solver_params* p, const double* xyz, const double* dom,
+                          aifmm_solver** out) {
   AIFMM_REQUIRE(k && p && out, AIFMM_EINVAL, "NULL argument");
   AIFMM_REQUIRE(p->precision >= 0 && p->precision <= 3, AIFMM_EINVAL,
                 "precision must be 0 (plain), 1, 2 or 3 (mixed)");
@@ -29,10 +30,44 @@ int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_sol
   const char* pt = std::getenv("AIFMM_PHASE_TIMES");
   sp.phaseTiming = pt && pt[0] == '1';
   std::unique_ptr<aifmm_solver> s(new aifmm_solver);
-  s->s.reset(new Solver(k, sp));
+  s->s.reset(new Solver(k, sp, xyz, dom));
   s->s->build();
   ctx_retain(k->ctx);
   *out = s.release();
+}
+
+int aifmm_solver_create(aifmm_kernel* k, const aifmm_solver_params* p, aifmm_solver** out) {
+  API_BEGIN
+  solver_create(k, p, nullptr, nullptr, out);
+  API_END
+}
+
+int aifmm_solver_create_at(aifmm_kernel* k, const aifmm_solver_params* p, const double* xyz, int n,
+                           const double domain[6], aifmm_solver** out) {
+  API_BEGIN
+  AIFMM_REQUIRE(k && xyz, AIFMM_EINVAL, "NULL argument");
+  AIFMM_REQUIRE(n == k->geom.N, AIFMM_EINVAL, "one location per unknown is required");
+  for (long i = 0; i < 3L * n; ++i) AIFMM_REQUIRE(std::isfinite(xyz[i]), AIFMM_EINVAL, "non-finite location");
+  if (domain)
+    for (int q = 0; q < 3; ++q)
+      AIFMM_REQUIRE(std::isfinite(domain[2 * q]) && std::isfinite(domain[2 * q + 1]) &&
+                        domain[2 * q] <= domain[2 * q + 1],
+                    AIFMM_EINVAL, "bad domain box");
+  solver_create(k, p, xyz, domain, out);
+  API_END
+}
+
+int aifmm_solver_tree_order(aifmm_solver* s, int* order) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && order, AIFMM_EINVAL, "NULL argument");
+  Solver& S = *s->s;
+  int pos = 0;
+  for (const DBox& B : S.tree[S.nLevels])
+    for (int id : B.chargeLocations) {
+      AIFMM_REQUIRE(pos < S.N, AIFMM_EINVAL, "leaves hold more unknowns than the kernel");
+      order[pos++] = id;
+    }
+  AIFMM_REQUIRE(pos == S.N, AIFMM_EINVAL, "leaves do not cover every unknown");
   API_END
 }
 

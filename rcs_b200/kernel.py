@@ -141,6 +141,30 @@ class EFIEMatrix(kernel):
         return out.view(np.complex128).copy()
 
 
+    def getJAtCentroids(self, coefficients) -> np.ndarray:
+        """Surface current at the triangle centroids, (n_tris, 3) complex:
+        EFIEMatrix::getJAtCentroids, src/EFIEMatrix.cpp:1100-1130 (on the GPU)."""
+        c = np.ascontiguousarray(np.asarray(coefficients, dtype=np.complex128).reshape(self.N)).view(np.float64)
+        out = np.zeros(6 * self.mesh.n_tris, dtype=np.float64)
+        _lib.check(_lib.lib().aifmm_kernel_currents(self.h, c, out))
+        return out.view(np.complex128).reshape(3, self.mesh.n_tris).T.copy()
+
+    def getRCS_OnePointQuadrature(self, theta, phi, J) -> np.ndarray:
+        """Bistatic RCS of centroid currents J at the angles (theta, phi)
+        (arrays of equal length, or scalars): EFIEMatrix::getRCS_OnePointQuadrature,
+        src/EFIEMatrix.cpp:916-930, all angles in one GPU launch."""
+        th = np.atleast_1d(np.asarray(theta, dtype=np.float64))
+        ph = np.broadcast_to(np.asarray(phi, dtype=np.float64), th.shape)
+        Jc = np.asarray(J, dtype=np.complex128)
+        if Jc.shape != (self.mesh.n_tris, 3):
+            raise ValueError("J must be (n_tris, 3)")
+        Jf = np.ascontiguousarray(Jc.T).view(np.float64).ravel()
+        out = np.zeros(th.size, dtype=np.float64)
+        _lib.check(_lib.lib().aifmm_kernel_rcs(self.h, Jf, th.size, np.ascontiguousarray(th),
+                                                np.ascontiguousarray(ph), out))
+        return out
+
+
 class ElectrostaticsMatrix(kernel):
     """Piecewise-constant collocation kernel, src/ElectrostaticsMatrix.cpp:48-52."""
 

@@ -46,11 +46,23 @@ class _TreeView:
 
 class AIFMM:
     def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 8, fillin_tol: int = 10,
-                 fillin_rank: int = 0, n_levels: int = 0, precision: int = 0, exact_rrqr: bool = False):
+                 fillin_rank: int = 0, n_levels: int = 0, precision: int = 0, exact_rrqr: bool = False,
+                 locations=None, domain=None):
+        """locations (N, 3) and domain (xmin, xmax, ymin, ymax, zmin, zmax) play
+        the parts of inputsToSolverClass::locations and xmin..zmax; by default
+        the tree is built over the kernel's own unknown locations."""
         p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(fillin_tol), int(fillin_rank), int(n_levels),
                               int(precision), int(bool(exact_rrqr)))
         h = C.c_void_p()
-        _lib.check(_lib.lib().aifmm_solver_create(K.h, C.byref(p), C.byref(h)))
+        if locations is None and domain is None:
+            _lib.check(_lib.lib().aifmm_solver_create(K.h, C.byref(p), C.byref(h)))
+        else:
+            loc = np.ascontiguousarray(K.locations() if locations is None else locations, dtype=np.float64)
+            if loc.shape != (K.N, 3):
+                raise ValueError("locations must be (N, 3)")
+            dom = None if domain is None else np.ascontiguousarray(domain, dtype=np.float64).reshape(6)
+            _lib.check(_lib.lib().aifmm_solver_create_at(K.h, C.byref(p), loc.ravel(), K.N,
+                                                          None if dom is None else dom.ctypes.data, C.byref(h)))
         self.h = h
         self.kernel = K
         self.N = K.N
@@ -123,6 +135,13 @@ class AIFMM:
                                                               C.c_void_p(x_ptr), float(tol), int(restart),
                                                               int(maxit), C.byref(gi)))
         return {f: getattr(gi, f) for f, _ in gi._fields_}
+
+    def tree_order(self) -> np.ndarray:
+        """order[p] = the unknown at position p of the tree-ordered solution
+        (FMM2DTree::getx before reorder)."""
+        out = np.zeros(self.N, dtype=np.int32)
+        _lib.check(_lib.lib().aifmm_solver_tree_order(self.h, out))
+        return out
 
     def info(self) -> dict:
         i = _lib.SolverInfo()
