@@ -48,7 +48,9 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   release();
   ctx = c;
   bytes = n;
+  const double t0 = opprof::enabled() ? opprof::now() : 0.0;
   cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
+  if (opprof::enabled()) opprof::add("pool_alloc", opprof::now() - t0);
   if (e == cudaErrorMemoryAllocation) {
     // the pool keeps freed blocks; return them to the device and retry once
     cudaGetLastError();
@@ -76,7 +78,11 @@ void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
   }
   const int c0 = (int)(head / aifmm_ctx::kRingChunk), c1 = (int)((head + n - 1) / aifmm_ctx::kRingChunk);
   for (int q = c0; q <= c1; ++q)  // a chunk from an earlier lap: its last copy must be done
-    if (c->ringChunkLap[q] != 0 && c->ringChunkLap[q] != c->ringLap) AIFMM_CUDA(cudaEventSynchronize(c->ringEvent[q]));
+    if (c->ringChunkLap[q] != 0 && c->ringChunkLap[q] != c->ringLap) {
+      const double t0 = opprof::enabled() ? opprof::now() : 0.0;
+      AIFMM_CUDA(cudaEventSynchronize(c->ringEvent[q]));
+      if (opprof::enabled()) opprof::add("ring_wait", opprof::now() - t0);
+    }
   std::memcpy(c->ring + head, src, n);
   AIFMM_CUDA(cudaMemcpyAsync(dst, c->ring + head, n, cudaMemcpyHostToDevice, c->stream));
   for (int q = c0; q <= c1; ++q) {
@@ -88,7 +94,9 @@ void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
 
 void DevBuf::release() {
   if (p && ctx) {
+    const double t0 = opprof::enabled() ? opprof::now() : 0.0;
     cudaFreeAsync(p, ctx->stream);
+    if (opprof::enabled()) opprof::add("pool_free", opprof::now() - t0);
     ctx->bytes_live -= bytes;
   }
   p = nullptr;
@@ -106,7 +114,8 @@ const char* aifmm_last_error(void) { return g_last_error.c_str(); }
 
 int aifmm_profile_ops(int on) {
   API_BEGIN
-  opprof::enable(on != 0);
+  AIFMM_REQUIRE(on >= 0 && on <= 2, AIFMM_EINVAL, "mode must be 0 (off), 1 (synchronising) or 2 (host time)");
+  opprof::enable(on);
   API_END
 }
 

@@ -8,18 +8,28 @@
 namespace aifmm {
 
 namespace opprof {
+static int g_mode = 0;
 static bool g_on = false;
 static std::mutex g_mu;
 static std::map<std::string, std::pair<long, double>> g_table;
-static double now() {
+double now() {
   return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
 }
-void enable(bool on) {
+void enable(int mode) {
   std::lock_guard<std::mutex> l(g_mu);
-  g_on = on;
+  g_mode = mode;
+  g_on = mode != 0;
   g_table.clear();
 }
 bool enabled() { return g_on; }
+int mode() { return g_mode; }
+cudaError_t sync(cudaStream_t s) {
+  if (!g_on) return cudaStreamSynchronize(s);
+  const double t0 = now();
+  const cudaError_t e = cudaStreamSynchronize(s);
+  add("sync_wait", now() - t0);
+  return e;
+}
 void add(const char* name, double seconds) {
   std::lock_guard<std::mutex> l(g_mu);
   auto& e = g_table[name];
@@ -39,7 +49,7 @@ std::string report() {
 Scope::Scope(const char* n, cudaStream_t s) : name(n), stream(s), t0(g_on ? now() : 0.0) {}
 Scope::~Scope() {
   if (!g_on) return;
-  cudaStreamSynchronize(stream);
+  if (g_mode == 1) cudaStreamSynchronize(stream);
   add(name, now() - t0);
 }
 }  // namespace opprof
@@ -220,7 +230,7 @@ std::vector<double> Ops::norms(const std::vector<const DMat*>& ms) const {
   znorm_grouped(ctx, ps, d.as<double>());
   std::vector<double> h(ps.size());
   AIFMM_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
-  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  AIFMM_CUDA(opprof::sync(ctx->stream));
   for (size_t q = 0; q < idx.size(); ++q) out[idx[q]] = h[q];
   return out;
 }
@@ -232,7 +242,7 @@ double Ops::maxColNorm(const DMat& a) const {
   znorm_grouped(ctx, ps, d.as<double>());
   std::vector<double> h(ps.size());
   AIFMM_CUDA(cudaMemcpyAsync(h.data(), d.p, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, ctx->stream));
-  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  AIFMM_CUDA(opprof::sync(ctx->stream));
   double best = -1.0;
   for (double v : h) best = std::max(best, v);
   return best;
@@ -255,7 +265,7 @@ DMat Ops::solve(const DLU& f, const DMat& b) const {
   if (x.size()) zgetrs(ctx, f.lu.p, f.n, f.lu.ld(), f.piv->as<int>(), x.p, x.c, x.ld());
   return x;
 }
-void Ops::sync() const { AIFMM_CUDA(cudaStreamSynchronize(ctx->stream)); }
+void Ops::sync() const { AIFMM_CUDA(opprof::sync(ctx->stream)); }
 std::vector<zd> Ops::download(const DMat& a) const {
   std::vector<zd> h((size_t)a.size());
   if (a.size())

@@ -11,13 +11,21 @@
 namespace aifmm {
 
 // Per-operation accounting of the host-driven factorization, for diagnosis:
-// off by default; when on, each instrumented scope synchronises the stream
-// on exit, so its time is host enqueue + device execution of that operation.
+// off by default.  Mode 1: each instrumented scope synchronises the stream on
+// exit, so its time is host enqueue + device execution of that operation.
+// Mode 2: scopes record host time only (no synchronisation), and the time the
+// host spends blocked on the device ("sync_wait") and in the memory pool
+// ("pool_alloc", "pool_free") is recorded too, which splits a host-driven
+// run into host work and waiting for the GPU.
 namespace opprof {
-void enable(bool on);
+void enable(int mode);
 bool enabled();
+int mode();
+double now();
 void add(const char* name, double seconds);
 std::string report();
+// cudaStreamSynchronize, accounted as "sync_wait" when profiling is on
+cudaError_t sync(cudaStream_t s);
 struct Scope {
   const char* name;
   cudaStream_t stream;

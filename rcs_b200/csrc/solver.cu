@@ -454,6 +454,7 @@ void Solver::build() {  // AIFMM.cpp:7-93
 
 // ------------------------------------------------------------ non-leaf P2P, T:3413-3504
 void Solver::initP2PNonLeaf(int j) {
+  opprof::Scope prof_fn_("nonleaf_p2p", ctx->stream);
   PhaseTimer pt(*this, stats.t_nonleaf);
   std::vector<CopyProblem> cps;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
@@ -586,6 +587,7 @@ DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int
 // empty partition 2 is the unit norm of the first old column.
 DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel,
                   bool* prefix) {
+  opprof::Scope prof_fn_("rrqr_total", ctx->stream);
   PhaseTimer pt(*this, stats.t_rrqr);
   const int m = A.r, n = A.c;
   stats.nRRQR++;
@@ -789,6 +791,7 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   DMat nL2P_k, nP2Mt_b, M2L_k_b, nL2P_b, nP2Mt_k, M2L_b_k;
   bool pkL, pbM, pbL, pkM;  // which new bases start with the old ones
   {
+  opprof::Scope prof_fn_("compress_p2p", ctx->stream);
     DMat a = tree[j][k].L2P, bb = tree[j][b].P2M, c = tree[j][k].P2P[b];
     compressP2PRRQR(j, k, b, a, bb, c, nL2P_k, nP2Mt_b, M2L_k_b, pkL, pbM);
   }
@@ -838,6 +841,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   Bk.maxPivot_L2P = std::max(Bk.maxPivot_L2P, mp);
   DMat M2L_k_b = ops.mul(nL2P_k, OP_C, Bk.M2P[b], OP_N);  // Rk'
   {
+  opprof::Scope prof_fn_("compress_p2l", ctx->stream);
     const DMat& M = Bk.M2L[b];
     if (pL) {  // Rk = [I; 0]: M2L[b] adds into the leading rows
       if (M.size() > 0)
@@ -890,6 +894,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
 // ------------------------------------------------------------ elimination
 // eliminate_x, T:3561-3611 with :3656-3791 (empty box) and :3800-4042.
 void Solver::eliminateX(int j, int k) {
+  opprof::Scope prof_fn_("elim_x", ctx->stream);
   PhaseTimer pt(*this, stats.t_elim_x);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };
@@ -1021,6 +1026,7 @@ void Solver::eliminateX(int j, int k) {
 
 // eliminate_z, T:4081-4113 with :4151-4296 (empty) and :4304-4509.
 void Solver::eliminateZ(int j, int k) {
+  opprof::Scope prof_fn_("elim_z", ctx->stream);
   PhaseTimer pt(*this, stats.t_elim_z);
   DBox& B = tree[j][k];
   auto E = [&](int x) { return tree[j][x].Eliminated; };

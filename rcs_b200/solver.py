@@ -215,9 +215,13 @@ def launch_count() -> int:
     return n.value
 
 
-def profile_ops(on: bool) -> None:
-    """Start (clear) or stop the per-operation accounting of the solver."""
-    _lib.check(_lib.lib().aifmm_profile_ops(int(bool(on))))
+def profile_ops(on) -> None:
+    """Start (clear) or stop the per-operation accounting of the solver:
+    False/0 off; True/1 every accounted operation synchronises (host enqueue +
+    device time); 2 host time only, plus the time blocked on the device
+    (sync_wait, ring_wait) and in the memory pool (pool_alloc, pool_free)."""
+    mode = 1 if on is True else (0 if on is False else int(on))
+    _lib.check(_lib.lib().aifmm_profile_ops(mode))
 
 
 def profile_ops_read() -> str:

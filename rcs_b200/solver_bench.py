@@ -3,7 +3,7 @@
     python -m rcs_b200.solver_bench [--sub 4] [--radius 0.15] [--freq 2e9] [--leaf 32]
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
                                     [--precision 0|1|2] [--op-tol 10] [--nrhs 8]
-                                    [--gmres 1e-6] [--profile-ops]
+                                    [--gmres 1e-6] [--profile-ops] [--profile-host]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
 AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
@@ -37,6 +37,8 @@ def main():
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--gmres", type=float, default=None)
     ap.add_argument("--profile-ops", action="store_true")
+    ap.add_argument("--profile-host", action="store_true",
+                    help="time the factorization with host-only accounting (no extra synchronisation)")
     a = ap.parse_args()
     from . import mesh as M
     from .kernel import EFIEMatrix
@@ -52,9 +54,20 @@ def main():
     if a.profile_ops:
         S.checkpoint()
     A = H2Operator(K, leaf_size=a.leaf, tol_pow=a.op_tol, n_levels=a.levels) if a.gmres else None
+    if a.profile_host:
+        from .solver import profile_ops
+        profile_ops(2)
     t0 = time.perf_counter()
     S.factorize()
     t_fac = time.perf_counter() - t0
+    if a.profile_host:
+        from .solver import profile_ops_read
+        rows = [ln.split() for ln in profile_ops_read().strip().splitlines()]
+        profile_ops(0)
+        print(f"# factorize: {t_fac:.3f} s, host-time accounting (inclusive scopes, no extra synchronisation)")
+        print("| operation | calls | host s |\n|---|---|---|")
+        for r in sorted(rows, key=lambda r: -float(r[2])):
+            print(f"| {r[0]} | {r[1]} | {float(r[2]):.3f} |")
     t0 = time.perf_counter()
     rec = None
     if A is not None:
