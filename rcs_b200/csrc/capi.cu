@@ -39,62 +39,24 @@ void ctx_release(aifmm_ctx* c) {
   for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
     if (c->ringEvent[i]) cudaEventDestroy(c->ringEvent[i]);
   if (c->ring) cudaFreeHost(c->ring);
-  ctx_cache_flush(c);
-  if (c->stream) cudaStreamSynchronize(c->stream);
   if (c->pool) cudaMemPoolDestroy(c->pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
 
-// Size classes of the block cache: 512 B, then four classes per power of two
-// (at most 25 % rounding).
-static size_t size_class(size_t n) {
-  if (n <= 512) return 512;
-  const int b = 63 - __builtin_clzll((unsigned long long)(n - 1));
-  const size_t step = (size_t)1 << (b - 2);
-  return (n + step - 1) / step * step;
-}
-
-void ctx_cache_flush(aifmm_ctx* c) {
-  std::lock_guard<std::mutex> l(c->cacheMu);
-  for (auto& kv : c->cache)
-    for (void* p : kv.second) cudaFreeAsync(p, c->stream);
-  c->cache.clear();
-  c->bytes_cached = 0;
-}
-
-// Blocks come from the context's cache of freed blocks of the same size class
-// when there is one, else from the stream-ordered pool; a pool allocation that
-// fails returns the cached blocks and the pool's reserve to the device and is
-// tried once more.  The cache replaces one pool allocation and one pool free
-// per block (a few microseconds of host time each, millions of times per
-// factorization) with a lookup.
 void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   release();
   ctx = c;
   bytes = n;
-  const size_t cls = size_class(n);
-  {
-    std::lock_guard<std::mutex> l(c->cacheMu);
-    auto it = c->cache.find(cls);
-    if (it != c->cache.end() && !it->second.empty()) {
-      p = it->second.back();
-      it->second.pop_back();
-      c->bytes_cached -= cls;
-      c->bytes_live += n;
-      return;
-    }
-  }
   const double t0 = opprof::enabled() ? opprof::now() : 0.0;
-  cudaError_t e = cudaMallocFromPoolAsync(&p, cls, c->pool, c->stream);
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
   if (opprof::enabled()) opprof::add("pool_alloc", opprof::now() - t0);
   if (e == cudaErrorMemoryAllocation) {
-    // return the cached blocks and the pool's reserve to the device, retry once
+    // the pool keeps freed blocks; return them to the device and retry once
     cudaGetLastError();
-    ctx_cache_flush(c);
     cudaStreamSynchronize(c->stream);
     cudaMemPoolTrimTo(c->pool, 0);
-    e = cudaMallocFromPoolAsync(&p, cls, c->pool, c->stream);
+    e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
   }
   if (e != cudaSuccess) {
     p = nullptr;
@@ -132,21 +94,9 @@ void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
 
 void DevBuf::release() {
   if (p && ctx) {
-    const size_t cls = size_class(bytes);
-    bool cached = false;
-    {
-      std::lock_guard<std::mutex> l(ctx->cacheMu);
-      if (!ctx->closed && ctx->bytes_cached + cls <= aifmm_ctx::kCacheCap) {
-        ctx->cache[cls].push_back(p);
-        ctx->bytes_cached += cls;
-        cached = true;
-      }
-    }
-    if (!cached) {
-      const double t0 = opprof::enabled() ? opprof::now() : 0.0;
-      cudaFreeAsync(p, ctx->stream);
-      if (opprof::enabled()) opprof::add("pool_free", opprof::now() - t0);
-    }
+    const double t0 = opprof::enabled() ? opprof::now() : 0.0;
+    cudaFreeAsync(p, ctx->stream);
+    if (opprof::enabled()) opprof::add("pool_free", opprof::now() - t0);
     ctx->bytes_live -= bytes;
   }
   p = nullptr;

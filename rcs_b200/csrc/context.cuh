@@ -2,9 +2,7 @@
 // pool, and the kernel (mesh) objects.
 #pragma once
 #include <memory>
-#include <mutex>
 #include <string>
-#include <unordered_map>
 #include <vector>
 
 #include "assemble.cuh"
@@ -34,21 +32,11 @@ struct aifmm_ctx {
   cudaEvent_t ringEvent[kRingChunks] = {};
   long ringChunkLap[kRingChunks] = {};  // 0: never used
   bool closed = false;
-  // Freed device blocks kept for reuse, by size class (see DevBuf::alloc).
-  // Every use of library memory is ordered on `stream`, so a block released
-  // by one operation can be handed to the next without an event: whatever
-  // reads it later was enqueued after whatever used it before.
-  std::mutex cacheMu;
-  std::unordered_map<size_t, std::vector<void*>> cache;
-  size_t bytes_cached = 0;
-  static constexpr size_t kCacheCap = (size_t)8 << 30;
 };
 
 namespace aifmm {
 void ctx_retain(aifmm_ctx* c);
 void ctx_release(aifmm_ctx* c);
-// Returns every cached block to the stream-ordered pool.
-void ctx_cache_flush(aifmm_ctx* c);
 }  // namespace aifmm
 
 namespace aifmm {
