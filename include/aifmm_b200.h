@@ -301,6 +301,10 @@ int aifmm_launch_count(long* n);
  * algorithmic flops (8 m n k per complex product) and launch count. */
 int aifmm_profile_gemm(int on);
 int aifmm_profile_gemm_read(double* ms, double* flops, long* launches);
+/* The device-time records of the GEMM profiler (grouped GEMM launches tagged
+ * "gemm:<precision>:<scope path>", RRQR launch chains "rrqr:<scope path>") as
+ * text lines "tag launches seconds flops", truncated to cap bytes. */
+int aifmm_profile_gemm_table(char* buf, int cap);
 
 #ifdef __cplusplus
 }

@@ -75,6 +75,7 @@ SIGNATURES = {
     "aifmm_solver_solve_gmres_device": (_i, [_p, _p, _p, _i, _p, _d, _i, _i, _p]),
     "aifmm_profile_gemm": (_i, [_i]),
     "aifmm_profile_gemm_read": (_i, [C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_long)]),
+    "aifmm_profile_gemm_table": (_i, [C.c_char_p, _i]),
 }
 
 

@@ -1,9 +1,12 @@
+#include <map>
+#include <tuple>
 // Dense complex128 kernels: grouped SIMT GEMM (64x64 tiles, 4x4 complex
 // micro-tiles per thread), blocked LU with a single-CTA panel, blocked
 // triangular solves, batched copies and norms.
 #include <algorithm>
 
 #include "dense.cuh"
+#include "dmat.cuh"
 
 namespace aifmm {
 
@@ -325,9 +328,13 @@ __global__ void __launch_bounds__(256) zgemm_tf32x3_kernel(const __grid_constant
 
 // Optional per-launch timing of the grouped GEMM (events on the launching
 // stream) for the roofline figure; off unless a caller enables it.
+// Each record carries the path of the instrumented scopes it was issued
+// from (opprof::path), so the time can be split by call site.
 struct GemmProfile {
   bool on = false;
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev;
+  std::vector<std::string> tag;
+  std::vector<double> fl;
   double flops = 0;
   long launches = 0;
 };
@@ -342,9 +349,19 @@ void gemm_profile_enable(bool on) {
   g_prof.on = on;
 }
 
+bool gemm_profile_on() { return g_prof.on; }
+
+void device_span_record(cudaEvent_t e0, cudaEvent_t e1, const std::string& tag, double flops) {
+  g_prof.ev.push_back({e0, e1});
+  g_prof.tag.push_back(tag);
+  g_prof.fl.push_back(flops);
+}
+
 void gemm_profile_read(double* ms, double* flops, long* launches) {
   double t = 0;
-  for (auto& e : g_prof.ev) {
+  for (size_t i = 0; i < g_prof.ev.size(); ++i) {
+    if (g_prof.tag[i].compare(0, 5, "gemm:") != 0) continue;
+    auto& e = g_prof.ev[i];
     AIFMM_CUDA(cudaEventSynchronize(e.second));
     float x = 0;
     AIFMM_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
@@ -353,6 +370,28 @@ void gemm_profile_read(double* ms, double* flops, long* launches) {
   *ms = t;
   *flops = g_prof.flops;
   *launches = g_prof.launches;
+}
+
+std::string gemm_profile_table() {
+  std::map<std::string, std::tuple<long, double, double>> by;
+  for (size_t i = 0; i < g_prof.ev.size(); ++i) {
+    auto& e = g_prof.ev[i];
+    AIFMM_CUDA(cudaEventSynchronize(e.second));
+    float x = 0;
+    AIFMM_CUDA(cudaEventElapsedTime(&x, e.first, e.second));
+    auto& r = by[g_prof.tag[i]];
+    std::get<0>(r)++;
+    std::get<1>(r) += x;
+    std::get<2>(r) += g_prof.fl[i];
+  }
+  std::string out;
+  char line[512];
+  for (auto& kv : by) {
+    snprintf(line, sizeof(line), "%s %ld %.6f %.6e\n", kv.first.c_str(), std::get<0>(kv.second),
+             std::get<1>(kv.second) / 1e3, std::get<2>(kv.second));
+    out += line;
+  }
+  return out;
 }
 
 // ------------------------------------------------------------------ GEMM, skinny split-K
@@ -559,7 +598,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
   AIFMM_LAUNCHED();
   if (g_prof.on) {
     AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
-    g_prof.ev.push_back({e0, e1});
+    device_span_record(e0, e1, "gemm:" + std::to_string(mode) + ":" + opprof::path(), flops);
     g_prof.flops += flops;
     g_prof.launches++;
   }

@@ -65,6 +65,12 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
 // Per-launch CUDA-event timing of zgemm_grouped (process-wide switch).
 void gemm_profile_enable(bool on);
 void gemm_profile_read(double* ms, double* flops, long* launches);
+// Device-time records (events around launches) while the GEMM profiler is
+// on: the grouped GEMMs and the RRQR launch chains; a table by tag of
+// "tag launches seconds flops" lines.
+bool gemm_profile_on();
+void device_span_record(cudaEvent_t e0, cudaEvent_t e1, const std::string& tag, double flops);
+std::string gemm_profile_table();
 
 struct CopyProblem {
   const zd* src;     // nullptr: dst is zero-filled

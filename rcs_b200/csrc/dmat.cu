@@ -46,8 +46,18 @@ std::string report() {
   }
   return out;
 }
-Scope::Scope(const char* n, cudaStream_t s) : name(n), stream(s), t0(g_on ? now() : 0.0) {}
+static thread_local std::vector<const char*> g_stack;
+std::string path() {
+  std::string out;
+  for (const char* n : g_stack) {
+    if (!out.empty()) out += '/';
+    out += n;
+  }
+  return out;
+}
+Scope::Scope(const char* n, cudaStream_t s) : name(n), stream(s), t0(g_on ? now() : 0.0) { g_stack.push_back(n); }
 Scope::~Scope() {
+  g_stack.pop_back();
   if (!g_on) return;
   if (g_mode == 1) cudaStreamSynchronize(stream);
   add(name, now() - t0);

@@ -26,6 +26,9 @@ void add(const char* name, double seconds);
 std::string report();
 // cudaStreamSynchronize, accounted as "sync_wait" when profiling is on
 cudaError_t sync(cudaStream_t s);
+// The names of the instrumented scopes open on this thread, outermost first,
+// joined by '/' (for tagging device-time records).
+std::string path();
 struct Scope {
   const char* name;
   cudaStream_t stream;

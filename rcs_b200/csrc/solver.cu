@@ -559,7 +559,17 @@ DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int
   P.istate = (int*)((char*)out.p + 16);
   P.dstate = (double*)((char*)out.p + 32);
   P.p2cap = p2cap;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (gemm_profile_on()) {
+    AIFMM_CUDA(cudaEventCreate(&e0));
+    AIFMM_CUDA(cudaEventCreate(&e1));
+    AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
+  }
   launch_rrqr_split(ctx, {P});
+  if (gemm_profile_on()) {
+    AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
+    device_span_record(e0, e1, "rrqr:" + opprof::path(), 0.0);
+  }
   stats.kernels += 4;
   struct {
     int rank, pad;

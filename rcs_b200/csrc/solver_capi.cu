@@ -1,6 +1,7 @@
 // C ABI of the AIFMM solver (see include/aifmm_b200.h).
 #include <cmath>
 #include <cstdlib>
+#include <cstring>
 #include <memory>
 
 #include "capi_guard.cuh"
@@ -167,6 +168,16 @@ int aifmm_profile_gemm_read(double* ms, double* flops, long* launches) {
   API_BEGIN
   AIFMM_REQUIRE(ms && flops && launches, AIFMM_EINVAL, "NULL argument");
   gemm_profile_read(ms, flops, launches);
+  API_END
+}
+
+int aifmm_profile_gemm_table(char* buf, int cap) {
+  API_BEGIN
+  AIFMM_REQUIRE(buf && cap > 0, AIFMM_EINVAL, "bad buffer");
+  const std::string r = gemm_profile_table();
+  const size_t n = std::min(r.size(), (size_t)cap - 1);
+  std::memcpy(buf, r.data(), n);
+  buf[n] = 0;
   API_END
 }
 

@@ -234,6 +234,19 @@ def profile_gemm(on: bool) -> None:
     _lib.check(_lib.lib().aifmm_profile_gemm(int(bool(on))))
 
 
+def profile_gemm_table() -> list[tuple[str, int, float, float]]:
+    """Device time by call site while the GEMM profiler is on: (tag, launches,
+    seconds, flops) for the grouped GEMMs ("gemm:<precision>:<scope path>") and
+    the RRQR launch chains ("rrqr:<scope path>")."""
+    buf = C.create_string_buffer(1 << 20)
+    _lib.check(_lib.lib().aifmm_profile_gemm_table(buf, len(buf)))
+    out = []
+    for ln in buf.value.decode().strip().splitlines():
+        tag, n, sec, fl = ln.rsplit(" ", 3)
+        out.append((tag, int(n), float(sec), float(fl)))
+    return out
+
+
 def profile_gemm_read() -> tuple[float, float, int]:
     ms, fl, n = C.c_double(), C.c_double(), C.c_long()
     _lib.check(_lib.lib().aifmm_profile_gemm_read(C.byref(ms), C.byref(fl), C.byref(n)))

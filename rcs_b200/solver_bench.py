@@ -3,7 +3,7 @@
     python -m rcs_b200.solver_bench [--sub 4] [--radius 0.15] [--freq 2e9] [--leaf 32]
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
                                     [--precision 0|1|2] [--op-tol 10] [--nrhs 8]
-                                    [--gmres 1e-6] [--profile-ops] [--profile-host]
+                                    [--gmres 1e-6] [--profile-ops] [--profile-host] [--profile-gemm]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
 AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
@@ -37,6 +37,8 @@ def main():
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--gmres", type=float, default=None)
     ap.add_argument("--profile-ops", action="store_true")
+    ap.add_argument("--profile-gemm", action="store_true",
+                    help="device time of the factorization's GEMM launches and RRQR chains by call site")
     ap.add_argument("--profile-host", action="store_true",
                     help="time the factorization with host-only accounting (no extra synchronisation)")
     a = ap.parse_args()
@@ -57,9 +59,21 @@ def main():
     if a.profile_host:
         from .solver import profile_ops
         profile_ops(2)
+    if a.profile_gemm:
+        from .solver import profile_gemm
+        profile_gemm(True)
     t0 = time.perf_counter()
     S.factorize()
     t_fac = time.perf_counter() - t0
+    if a.profile_gemm:
+        from .solver import profile_gemm, profile_gemm_table
+        rows = profile_gemm_table()
+        profile_gemm(False)
+        tot = sum(r[2] for r in rows)
+        print(f"# factorize: {t_fac:.3f} s; device time of the recorded launches {tot:.3f} s")
+        print("| call site | launches | device s | TFLOP/s |\n|---|---|---|---|")
+        for tag, n, sec, fl in sorted(rows, key=lambda r: -r[2]):
+            print(f"| {tag} | {n} | {sec:.3f} | {fl / sec / 1e12 if sec > 0 and fl > 0 else 0:.1f} |")
     if a.profile_host:
         from .solver import profile_ops_read
         rows = [ln.split() for ln in profile_ops_read().strip().splitlines()]
