@@ -135,6 +135,37 @@ DMat Ops::alloc(int r, int c) const {
   }
   return m;
 }
+std::vector<DMat> Ops::allocMany(const std::vector<std::pair<int, int>>& shapes) const {
+  opprof::Scope prof_("alloc_many", ctx->stream);
+  constexpr size_t kAlign = 512 / sizeof(zd), kSlab = ((size_t)16 << 20) / sizeof(zd);
+  std::vector<DMat> out(shapes.size());
+  size_t i = 0;
+  while (i < shapes.size()) {
+    // the matrices [i, j) share one slab
+    size_t j = i, words = 0;
+    for (; j < shapes.size(); ++j) {
+      AIFMM_REQUIRE(shapes[j].first >= 0 && shapes[j].second >= 0, AIFMM_EINVAL, "negative matrix size");
+      const size_t w = ((size_t)shapes[j].first * shapes[j].second + kAlign - 1) / kAlign * kAlign;
+      if (j > i && words + w > kSlab) break;
+      words += w;
+    }
+    std::shared_ptr<DevBuf> slab;
+    if (words > 0) slab = std::make_shared<DevBuf>(ctx, sizeof(zd) * words);
+    size_t off = 0;
+    for (size_t q = i; q < j; ++q) {
+      DMat& m = out[q];
+      m.r = shapes[q].first;
+      m.c = shapes[q].second;
+      if (m.size() > 0) {
+        m.buf = slab;
+        m.p = slab->as<zd>() + off;
+        off += ((size_t)m.size() + kAlign - 1) / kAlign * kAlign;
+      }
+    }
+    i = j;
+  }
+  return out;
+}
 DMat Ops::zeros(int r, int c) const {
   opprof::Scope prof_("zeros", ctx->stream);
   DMat m = alloc(r, c);

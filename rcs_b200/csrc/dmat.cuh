@@ -63,6 +63,11 @@ struct Ops {
   aifmm_ctx* ctx;
   explicit Ops(aifmm_ctx* c) : ctx(c) {}
   DMat alloc(int r, int c) const;
+  // Several matrices carved out of shared device allocations (slabs of up to
+  // 16 MB, each matrix 512-byte aligned): one pool allocation per slab
+  // instead of one per matrix.  A slab's memory returns to the pool when the
+  // last matrix in it is released.
+  std::vector<DMat> allocMany(const std::vector<std::pair<int, int>>& shapes) const;
   DMat zeros(int r, int c) const;
   DMat ident(int n, zd d) const;
   DMat copy(const DMat& a) const;

@@ -633,8 +633,12 @@ DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank,
 void Solver::resizeRows(const std::vector<DMat*>& blocks, int rows) {
   std::vector<CopyProblem> cps;
   std::vector<DMat> keep;  // the old blocks stay alive until the copy is enqueued
-  for (DMat* b : blocks) {
-    DMat nw = ops.alloc(rows, b->c);
+  std::vector<std::pair<int, int>> shapes;
+  for (DMat* b : blocks) shapes.push_back({rows, b->c});
+  std::vector<DMat> fresh = ops.allocMany(shapes);
+  for (size_t q = 0; q < blocks.size(); ++q) {
+    DMat* b = blocks[q];
+    DMat nw = fresh[q];
     const int kept = std::min(rows, b->r);
     if (kept > 0 && b->c > 0) cps.push_back({b->p, nw.p, kept, b->c, b->ld(), nw.ld(), 0, ONE});
     if (rows > kept && b->c > 0) cps.push_back({nullptr, nw.p + kept, rows - kept, b->c, 1, nw.ld(), 0, ONE});
@@ -647,8 +651,12 @@ void Solver::resizeRows(const std::vector<DMat*>& blocks, int rows) {
 void Solver::resizeCols(const std::vector<DMat*>& blocks, int cols) {
   std::vector<CopyProblem> cps;
   std::vector<DMat> keep;
-  for (DMat* b : blocks) {
-    DMat nw = ops.alloc(b->r, cols);
+  std::vector<std::pair<int, int>> shapes;
+  for (DMat* b : blocks) shapes.push_back({b->r, cols});
+  std::vector<DMat> fresh = ops.allocMany(shapes);
+  for (size_t q = 0; q < blocks.size(); ++q) {
+    DMat* b = blocks[q];
+    DMat nw = fresh[q];
     const int kept = std::min(cols, b->c);
     if (kept > 0 && b->r > 0) cps.push_back({b->p, nw.p, b->r, kept, b->ld(), nw.ld(), 0, ONE});
     if (cols > kept && b->r > 0)
@@ -676,9 +684,13 @@ void Solver::updateOtherM2LsAtK(int j, int k, int b, const DMat& nL2P, bool pref
   const DMat T = ops.mul(nL2P, OP_C, B.L2P, OP_N);
   GemmBatch g;
   std::vector<DMat> keep;  // old blocks stay alive until the batched GEMM that reads them is launched
-  for (DMat* old : blocks) {
+  std::vector<std::pair<int, int>> shapes;
+  for (DMat* old : blocks) shapes.push_back({T.r, old->c});
+  std::vector<DMat> fresh = ops.allocMany(shapes);
+  for (size_t q = 0; q < blocks.size(); ++q) {
+    DMat* old = blocks[q];
     keep.push_back(*old);
-    DMat nw = ops.alloc(T.r, old->c);
+    DMat nw = fresh[q];
     if (T.c == 0) nw = ops.zeros(T.r, old->c);
     else g.add(nw, T, OP_N, *old, OP_N, ONE, ZERO);
     *old = nw;
@@ -703,9 +715,13 @@ void Solver::updateOtherM2LsAtB(int j, int k, int b, const DMat& nP2Mt, bool pre
   const DMat S = ops.mul(Bb.P2M, OP_N, nP2Mt, OP_N);
   GemmBatch g;
   std::vector<DMat> keep;
-  for (DMat* old : blocks) {
+  std::vector<std::pair<int, int>> shapes;
+  for (DMat* old : blocks) shapes.push_back({old->r, S.c});
+  std::vector<DMat> fresh = ops.allocMany(shapes);
+  for (size_t q = 0; q < blocks.size(); ++q) {
+    DMat* old = blocks[q];
     keep.push_back(*old);
-    DMat nw = ops.alloc(old->r, S.c);
+    DMat nw = fresh[q];
     if (S.r == 0) nw = ops.zeros(old->r, S.c);
     else g.add(nw, *old, OP_N, S, OP_N, ONE, ZERO);
     *old = nw;
