@@ -50,7 +50,12 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   bytes = n;
   const double t0 = opprof::enabled() ? opprof::now() : 0.0;
   cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
-  if (opprof::enabled()) opprof::add("pool_alloc", opprof::now() - t0);
+  if (opprof::enabled()) {
+    const double dt = opprof::now() - t0;
+    opprof::add("pool_alloc", dt);
+    opprof::add(n < ((size_t)1 << 20) ? "pool_alloc_lt1MB" : n < ((size_t)64 << 20) ? "pool_alloc_lt64MB" : "pool_alloc_ge64MB",
+                dt);
+  }
   if (e == cudaErrorMemoryAllocation) {
     // the pool keeps freed blocks; return them to the device and retry once
     cudaGetLastError();
