@@ -39,15 +39,37 @@ void ctx_release(aifmm_ctx* c) {
   for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
     if (c->ringEvent[i]) cudaEventDestroy(c->ringEvent[i]);
   if (c->ring) cudaFreeHost(c->ring);
+  if (c->arena) {
+    for (auto& ch : c->arena->chunks()) cudaFreeAsync((void*)ch.first, c->stream);
+    c->arena.reset();
+    if (c->stream) cudaStreamSynchronize(c->stream);
+  }
   if (c->pool) cudaMemPoolDestroy(c->pool);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
+}
+
+// Returns the arena's chunks that hold no block to the pool.
+static void arena_trim(aifmm_ctx* c) {
+  if (!c->arena) return;
+  std::lock_guard<std::mutex> l(c->arenaMu);
+  for (auto& ch : c->arena->takeFreeChunks()) cudaFreeAsync((void*)ch.first, c->stream);
 }
 
 void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   release();
   ctx = c;
   bytes = n;
+  if (c->arena && n >= Arena::kMinSize) {
+    std::lock_guard<std::mutex> l(c->arenaMu);
+    const uint64_t a = c->arena->alloc(n);
+    if (a != 0) {
+      p = (void*)a;
+      fromArena = true;
+      c->bytes_live += n;
+      return;
+    }
+  }
   const double t0 = opprof::enabled() ? opprof::now() : 0.0;
   cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
   if (opprof::enabled()) {
@@ -57,8 +79,9 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
                 dt);
   }
   if (e == cudaErrorMemoryAllocation) {
-    // the pool keeps freed blocks; return them to the device and retry once
+    // the pool and the arena keep freed blocks; return them to the device and retry once
     cudaGetLastError();
+    arena_trim(c);
     cudaStreamSynchronize(c->stream);
     cudaMemPoolTrimTo(c->pool, 0);
     e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
@@ -119,6 +142,17 @@ void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
 }
 
 void DevBuf::release() {
+  if (p && ctx && fromArena) {
+    {
+      std::lock_guard<std::mutex> l(ctx->arenaMu);
+      ctx->arena->release((uint64_t)p);
+    }
+    ctx->bytes_live -= bytes;
+    p = nullptr;
+    bytes = 0;
+    fromArena = false;
+    return;
+  }
   if (p && ctx) {
     const double t0 = opprof::enabled() ? opprof::now() : 0.0;
     cudaFreeAsync(p, ctx->stream);
@@ -186,6 +220,17 @@ int aifmm_ctx_create(int device, aifmm_ctx** out) {
   uint64_t thresh = UINT64_MAX;  // keep freed blocks for reuse
   AIFMM_CUDA(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &thresh));
   AIFMM_CUDA(cudaMallocHost((void**)&c->ring, aifmm_ctx::kRingBytes));
+  {
+    aifmm_ctx* cp = c.get();
+    c->arena.reset(new Arena([cp](size_t bytes) -> uint64_t {
+      void* q = nullptr;
+      if (cudaMallocFromPoolAsync(&q, bytes, cp->pool, cp->stream) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+      }
+      return (uint64_t)q;
+    }));
+  }
   for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
     AIFMM_CUDA(cudaEventCreateWithFlags(&c->ringEvent[i], cudaEventDisableTiming));
   *out = c.release();

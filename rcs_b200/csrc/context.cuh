@@ -2,9 +2,11 @@
 // pool, and the kernel (mesh) objects.
 #pragma once
 #include <memory>
+#include <mutex>
 #include <string>
 #include <vector>
 
+#include "arena.cuh"
 #include "assemble.cuh"
 
 // Objects created on a context (kernels, solvers) hold a reference; the
@@ -32,6 +34,10 @@ struct aifmm_ctx {
   cudaEvent_t ringEvent[kRingChunks] = {};
   long ringChunkLap[kRingChunks] = {};  // 0: never used
   bool closed = false;
+  // Sub-allocator for the blocks of 256 KB and more (arena.cuh); its chunks
+  // come from `pool`.  Created with the context.
+  std::mutex arenaMu;
+  std::unique_ptr<aifmm::Arena> arena;
 };
 
 namespace aifmm {
@@ -46,16 +52,21 @@ struct DevBuf {
   aifmm_ctx* ctx = nullptr;
   void* p = nullptr;
   size_t bytes = 0;
+  bool fromArena = false;  // p came from the context's arena, not the pool
   DevBuf() {}
   DevBuf(aifmm_ctx* c, size_t n) { alloc(c, n); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), bytes(o.bytes) { o.p = nullptr; o.bytes = 0; }
+  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), bytes(o.bytes), fromArena(o.fromArena) {
+    o.p = nullptr;
+    o.bytes = 0;
+    o.fromArena = false;
+  }
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
-      ctx = o.ctx; p = o.p; bytes = o.bytes;
-      o.p = nullptr; o.bytes = 0;
+      ctx = o.ctx; p = o.p; bytes = o.bytes; fromArena = o.fromArena;
+      o.p = nullptr; o.bytes = 0; o.fromArena = false;
     }
     return *this;
   }
