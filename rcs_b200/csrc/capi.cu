@@ -93,27 +93,6 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   }
   c->bytes_live += n;
 }
-// Keeps at least `bytes` of mapped but unused memory in the context's pool
-// (allocated once and freed, so the pool retains it): later allocations are
-// carved from it instead of mapping new memory, which costs milliseconds per
-// large request.  Best effort: a failed reservation changes nothing.
-void ctx_reserve(aifmm_ctx* c, size_t bytes) {
-  size_t reserved = 0, used = 0;
-  if (cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrReservedMemCurrent, &reserved) != cudaSuccess ||
-      cudaMemPoolGetAttribute(c->pool, cudaMemPoolAttrUsedMemCurrent, &used) != cudaSuccess) {
-    cudaGetLastError();
-    return;
-  }
-  const size_t spare = reserved > used ? reserved - used : 0;
-  if (spare >= bytes) return;
-  void* p = nullptr;
-  if (cudaMallocFromPoolAsync(&p, bytes - spare, c->pool, c->stream) != cudaSuccess) {
-    cudaGetLastError();
-    return;
-  }
-  cudaFreeAsync(p, c->stream);
-}
-
 void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
   if (n == 0) return;
   if (!c->ring || n > aifmm_ctx::kRingBytes / 4) {

@@ -77,9 +77,6 @@ struct DevBuf {
   T* as() const { return static_cast<T*>(p); }
 };
 
-// Keeps at least `bytes` of mapped, unused memory in the context's pool.
-void ctx_reserve(aifmm_ctx* c, size_t bytes);
-
 // Asynchronous host-to-device copy of n bytes on the context stream, staged
 // through the pinned ring when it fits (see aifmm_ctx).
 void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n);

@@ -1190,11 +1190,6 @@ void Solver::eliminateZ(int j, int k) {
 void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   const double t0 = wall();
   AIFMM_CUDA(cudaSetDevice(ctx->device));
-  {  // the factorization allocates and frees blocks of every size: give the pool room first
-    size_t freeB = 0, totalB = 0;
-    AIFMM_CUDA(cudaMemGetInfo(&freeB, &totalB));
-    ctx_reserve(ctx, std::min(freeB / 2, (size_t)32 << 30));
-  }
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
   stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
