@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "factor+solve s at rel. residual 1e-6: mixed/batched/learned vs plain FP64 GPU"
 
-# Workloads; synthetic icosphere meshes, seeded plane waves.
+# Workloads (the benchmark configurations); synthetic icosphere meshes, seeded plane waves.
 # tol_pow / fillin_tol: the factorization's ACA and RRQR tolerances; op_tol:
 # ACA tolerance of the FP64 H^2 forward operator that GMRES iterates on; gmres:
 # target relative residual (None = direct solve only, the reference's path).

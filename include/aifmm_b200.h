@@ -35,7 +35,7 @@ extern "C" {
 #define AIFMM_ETIMEOUT (-4)  /* a bounded device wait gave up */
 #define AIFMM_ESTATE (-5)    /* call out of order (e.g. solve before factorize) */
 #define AIFMM_ESINGULAR (-6) /* exactly singular pivot met */
-#define AIFMM_ENOTIMPL (-7)  /* feature not available in this build */
+#define AIFMM_ENOTIMPL (-7)  /* feature not available in this library */
 #define AIFMM_EOVERFLOW (-8) /* a workspace bound was exceeded */
 
 typedef struct aifmm_ctx aifmm_ctx;

@@ -27,7 +27,7 @@ def mesh78(gold):
 
 
 def test_fixture_rwg_count(mesh78):
-    # 78 triangles of a closed sphere -> 117 interior edges (SURVEY C19).
+    # 78 triangles of a closed sphere -> 117 interior edges.
     assert M.rwg_count(mesh78) == 117
     K = oracle.EFIE(mesh78, 1.0e7)
     assert K.N == 117
