@@ -103,7 +103,7 @@ static void rrqr_host(aifmm_ctx* ctx, const double* A, int m, int n, int partiti
   P.rank = out.as<int>();
   P.maxPivot = (double*)((char*)out.p + 8);
   P.istate = (int*)((char*)out.p + 16);
-  P.dstate = (double*)((char*)out.p + 32);
+  P.dstate = (double*)((char*)out.p + 48);  // after the 8 ints of istate
   P.p2cap = -1;
   launch_rrqr_split(ctx, {P});
   struct {

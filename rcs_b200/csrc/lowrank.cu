@@ -429,6 +429,11 @@ void launch_rrqr(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
 // ------------------------------------------------------------------ RRQR, split
 namespace aifmm {
 
+// Partition 2 runs as per-step launches when it has at most this many steps
+// (the solver's fill-in recompressions have 5 to 11); longer runs keep the
+// single-CTA panel kernel.
+constexpr int kRRQRStepLaunchMax = 32;
+
 // One pivoting step at position j: pivot among positions [j, end), reflector
 // applied to (and norms downdated for) positions [j, applyEnd).  Same
 // arithmetic as the step of rrqr_kernel.  Returns false on the stop test.
@@ -518,6 +523,165 @@ __device__ bool rrqr_step_dev(const RRQRProblem& P, int j, int end, int applyEnd
   nref++;
   __syncthreads();
   return true;
+}
+
+// ---- partition 2 as one launch pair per step (pivot/reflector on one CTA,
+// reflector application one warp per column across the GPU).  The arithmetic
+// of each column is the same as in rrqr_step_dev, so the result equals the
+// single-CTA panel bit for bit.  State between launches lives in istate
+// ([0] committed reflectors, [1] rank of partition 1, [4] done, [5] partition-2
+// commits, [6] position of the step to apply or -1, [7] its reflector) and
+// dstate ([0] first pivot of partition 1, [1] maxPivot).  A step after the stop
+// (or past the step bound) returns at once.
+
+__device__ inline void rrqr_p2_bounds(const RRQRProblem& P, int& first, int& steps) {
+  const int rank_p1 = P.istate[1];
+  first = rank_p1;
+  steps = min(P.m, P.n) - (P.partition - rank_p1);
+  if (P.p2cap >= 0) steps = min(steps, first + P.p2cap);
+}
+
+__global__ void rrqr_p2_init_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.x];
+  for (int q = P.istate[1] + threadIdx.x; q < P.partition; q += blockDim.x) P.nsq[q] = 0.0;
+  if (threadIdx.x == 0) {
+    P.istate[4] = 0;
+    P.istate[5] = 0;
+    P.istate[6] = -1;
+    P.istate[7] = 0;
+  }
+}
+
+__global__ void __launch_bounds__(QR_NT) rrqr_p2_pivot_kernel(const RRQRProblem* __restrict__ probs, int t) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  const RRQRProblem P = probs[blockIdx.x];
+  const int tid = threadIdx.x, m = P.m, n = P.n;
+  if (P.istate[4]) {  // stopped earlier: nothing to apply
+    if (tid == 0) P.istate[6] = -1;
+    return;
+  }
+  int first, steps;
+  rrqr_p2_bounds(P, first, steps);
+  const int j = first + t;
+  if (j >= steps) {
+    if (tid == 0) {
+      P.istate[4] = 1;
+      P.istate[6] = -1;
+    }
+    return;
+  }
+  const int nref = P.istate[0];
+  double maxPivot = P.dstate[1];
+  zd* R = P.R;
+  // pivot, Householder vector and stop test: the first half of rrqr_step_dev
+  double bv = -1.0;
+  int bi = -1;
+  for (int q = j + tid; q < n; q += QR_NT) {
+    const double v = P.nsq[q];
+    if (bi < 0 || v > bv) { bv = v; bi = q; }
+  }
+  double mv;
+  int pos;
+  block_argmax<QR_NT>(bv, bi, shv, shi, mv, pos);
+  if (tid == 0 && pos != j) {
+    double tt = P.nsq[j]; P.nsq[j] = P.nsq[pos]; P.nsq[pos] = tt;
+    int u = P.perm[j]; P.perm[j] = P.perm[pos]; P.perm[pos] = u;
+  }
+  __syncthreads();
+  const int c = P.perm[j];
+  zd* x = R + (size_t)c * m;
+  double s = 0.0;
+  for (int i = j + tid; i < m; i += QR_NT) s += zabs2(x[i]);
+  const double xn = sqrt(block_sum<QR_NT>(s, shv));
+  zd* h = P.H + (size_t)nref * m;
+  if (tid == 0) {
+    const zd xj = x[j];
+    zd add;
+    if (P.realMode) add = zmk((xj.x >= 0 ? 1.0 : -1.0) * xn, 0.0);
+    else {
+      double sn, cs;
+      sincos(atan2(xj.y, xj.x), &sn, &cs);
+      add = zmk(cs * xn, sn * xn);
+    }
+    s_alpha = zadd(xj, add);
+  }
+  __syncthreads();
+  double s2 = 0.0;
+  for (int i = tid; i < m; i += QR_NT) {
+    zd v = (i < j) ? zmk(0, 0) : ((i == j) ? s_alpha : x[i]);
+    h[i] = v;
+    s2 += zabs2(v);
+  }
+  const double hn = sqrt(block_sum<QR_NT>(s2, shv));
+  __syncthreads();
+  if (hn > 0) {
+    const double r2 = sqrt(2.0);
+    for (int i = j + tid; i < m; i += QR_NT) h[i] = zmk((h[i].x * r2) / hn, (h[i].y * r2) / hn);
+  }
+  __syncthreads();
+  zd w = zmk(0, 0);
+  for (int i = j + tid; i < m; i += QR_NT) w = zadd(w, zcmul(h[i], x[i]));
+  double wr = block_sum<QR_NT>(w.x, shv);
+  double wi = block_sum<QR_NT>(w.y, shv);
+  const zd rjj = zsub(x[j], zmul(h[j], zmk(wr, wi)));
+  const double pivot = zabs(rjj);
+  if (j == first) maxPivot = fmax(P.inputPivot, pivot);
+  const bool stop = (pivot / maxPivot < P.tol2 || j - first >= P.fillInRank);
+  if (tid == 0) {
+    P.dstate[1] = maxPivot;
+    if (stop) {
+      P.istate[4] = 1;
+      P.istate[6] = -1;
+    } else {
+      P.istate[6] = j;
+      P.istate[7] = nref;
+      P.istate[0] = nref + 1;
+      P.istate[5] += 1;
+    }
+  }
+}
+
+// The committed reflector of the step applied to the columns at positions
+// >= j, one warp per column, with the pivot column's sub-diagonal zeroed and
+// the downdates of the norms at positions > j.
+__global__ void rrqr_p2_apply_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int j = P.istate[6];
+  if (j < 0) return;
+  const int m = P.m, lane = threadIdx.x & 31;
+  const int q = j + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= P.n) return;
+  const zd* h = P.H + (size_t)P.istate[7] * m;
+  zd* y = P.R + (size_t)P.perm[q] * m;
+  zd a = zmk(0, 0);
+  for (int i = j + lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
+  for (int o = 16; o > 0; o >>= 1) {
+    a.x += __shfl_xor_sync(0xffffffff, a.x, o);
+    a.y += __shfl_xor_sync(0xffffffff, a.y, o);
+  }
+  for (int i = j + lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
+  __syncwarp();
+  if (q == j) {
+    for (int i = j + 1 + lane; i < m; i += 32) y[i] = zmk(0, 0);
+  } else if (lane == 0) {
+    const double ab = zabs(y[j]);
+    P.nsq[q] = P.nsq[q] - ab * ab;
+  }
+}
+
+__global__ void rrqr_p2_finish_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.x];
+  if (threadIdx.x != 0) return;
+  int first, steps;
+  rrqr_p2_bounds(P, first, steps);
+  const int rank_p2 = (steps - first <= 0) ? min(steps - first, P.m) : P.istate[5];
+  const int rank = P.istate[1] + rank_p2;
+  P.istate[2] = P.istate[0];
+  P.istate[3] = rank;
+  *P.rank = rank;
+  *P.maxPivot = P.dstate[1];
 }
 
 // Partition 1 on the old-basis panel (positions [0, partition)).
@@ -645,14 +809,39 @@ void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
     maxCols = std::max(maxCols, std::min(p.m, p.n));
   }
   AIFMM_REQUIRE(probs.size() <= 65535, AIFMM_EINVAL, "too many RRQR problems in one launch");
+  // partition-2 steps to launch: at most fillInRank commits plus the step that
+  // stops, at most p2cap steps, at most min(m, n) positions
+  int p2steps = 0;
+  for (const RRQRProblem& p : probs) {
+    long t = (long)p.fillInRank + 1;
+    if (p.p2cap >= 0) t = std::min<long>(t, p.p2cap);
+    t = std::min<long>(t, std::min(p.m, p.n));
+    p2steps = std::max(p2steps, (int)std::max<long>(t, 0));
+  }
   DevBuf dp = upload(ctx, probs);
   const unsigned np = (unsigned)probs.size();
   rrqr_p1_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
   AIFMM_LAUNCHED();
   rrqr_fill_kernel<<<dim3((maxFill + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
   AIFMM_LAUNCHED();
-  rrqr_p2_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
-  AIFMM_LAUNCHED();
+  if (p2steps <= kRRQRStepLaunchMax) {
+    // one launch pair per step: the column updates spread over the GPU
+    int maxApply = 1;
+    for (const RRQRProblem& p : probs) maxApply = std::max(maxApply, p.n);
+    rrqr_p2_init_kernel<<<np, 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+    AIFMM_LAUNCHED();
+    for (int t = 0; t < p2steps; ++t) {
+      rrqr_p2_pivot_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>(), t);
+      AIFMM_LAUNCHED();
+      rrqr_p2_apply_kernel<<<dim3((maxApply + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+      AIFMM_LAUNCHED();
+    }
+    rrqr_p2_finish_kernel<<<np, 32, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+    AIFMM_LAUNCHED();
+  } else {
+    rrqr_p2_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
+    AIFMM_LAUNCHED();
+  }
   rrqr_q_kernel<<<dim3((maxCols + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());
   AIFMM_LAUNCHED();
 }

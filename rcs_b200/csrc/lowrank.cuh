@@ -41,7 +41,7 @@ struct RRQRProblem {
   zd* Q;             // out: m x rank (ld = m), space for m x (min(m,n)+1)
   int* rank;         // out
   double* maxPivot;  // out
-  int* istate;       // split pipeline only: 4 ints of scratch
+  int* istate;       // split pipeline only: 8 ints of scratch
   double* dstate;    // split pipeline only: 2 doubles of scratch
   int p2cap;         // split pipeline only: at most this many partition-2 steps (-1: no cap)
 };

@@ -557,7 +557,7 @@ DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int
   P.rank = (int*)out.p;
   P.maxPivot = (double*)((char*)out.p + 8);
   P.istate = (int*)((char*)out.p + 16);
-  P.dstate = (double*)((char*)out.p + 32);
+  P.dstate = (double*)((char*)out.p + 48);  // after the 8 ints of istate
   P.p2cap = p2cap;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   if (gemm_profile_on()) {
