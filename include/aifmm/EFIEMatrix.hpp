@@ -81,10 +81,10 @@ class EFIEMatrix : public kernel {
     for (size_t i = 0; i < patchList.size(); ++i) {
       const int v[3] = {patchList[i].indexOfVertex1, patchList[i].indexOfVertex2, patchList[i].indexOfVertex3};
       for (int e = 0; e < 3; ++e) {
-        const int a = v[e], b = v[(e + 1) % 3];
+        const int va = v[e], vb = v[(e + 1) % 3];
         Edge edge;
-        edge.indicesOfNodes = a < b ? std::make_pair(a, b) : std::make_pair(b, a);
-        edge.length = (nodeList[a] - nodeList[b]).norm();
+        edge.indicesOfNodes = va < vb ? std::make_pair(va, vb) : std::make_pair(vb, va);
+        edge.length = (nodeList[va] - nodeList[vb]).norm();
         edgeList.insert(edge);
         auto it = edge2PatchMap.find(edge.indicesOfNodes);
         if (it == edge2PatchMap.end()) {
@@ -145,6 +145,7 @@ class EFIEMatrix : public kernel {
   // dense LU solution (EFIEMatrix.cpp:831-837): the whole matrix is assembled
   // and factorized on the GPU
   void getCoefficients(Eigen::VectorXcd& rhs, Eigen::VectorXcd& coefficients) {
+    if (rhs.size() != N) throw std::runtime_error("aifmm: right-hand side length differs from N");
     std::vector<int> ids((size_t)N);
     for (int i = 0; i < N; ++i) ids[(size_t)i] = i;
     std::vector<std::complex<double>> Z((size_t)N * N), b = aifmm_dropin::to_c128(rhs), x((size_t)N);
@@ -155,6 +156,7 @@ class EFIEMatrix : public kernel {
   }
   // current at the triangle centroids (EFIEMatrix.cpp:1100-1130)
   void getJAtCentroids(Eigen::VectorXcd& coefficients, Eigen::MatrixXcd& JAtCentroids) {
+    if (coefficients.size() != N) throw std::runtime_error("aifmm: coefficient vector length differs from N");
     std::vector<std::complex<double>> cvec = aifmm_dropin::to_c128(coefficients);
     std::vector<std::complex<double>> J(patchList.size() * 3);
     aifmm_dropin::check(aifmm_kernel_currents(handle, reinterpret_cast<double*>(cvec.data()),
