@@ -74,6 +74,7 @@ class ElectrostaticsMatrix : public kernel {
   }
   // total charge = sum of density x area (ElectrostaticsMatrix.cpp:366-372)
   double getCapacitance(Eigen::VectorXd& chargeDensity) {
+    if (chargeDensity.size() != N) throw std::runtime_error("aifmm: charge density length differs from N");
     double q = 0.0;
     for (int i = 0; i < N; ++i) q += chargeDensity(i) * patchList[(size_t)i].area;
     return q;
@@ -87,6 +88,8 @@ class ElectrostaticsMatrix : public kernel {
   // C(i, j) = charge on conductor i+1 for 1 V on conductor j+1 (:383-402).
   // The reference accumulates into an uninitialised matrix; it starts from 0.
   void getCapacitanceMatrix(Eigen::MatrixXd chargeDensityMatrix, Eigen::MatrixXd& capacitanceMatrix) {
+    if (chargeDensityMatrix.rows() != N || chargeDensityMatrix.cols() < numConductors)
+      throw std::runtime_error("aifmm: charge densities must be N x (number of conductors)");
     capacitanceMatrix = Eigen::MatrixXd::Zero(numConductors, numConductors);
     for (int j = 0; j < numConductors; ++j)
       for (int k = 0; k < N; ++k) {
