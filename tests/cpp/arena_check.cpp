@@ -2,7 +2,9 @@
 // (rcs_b200/csrc/arena.cuh) with fake chunk addresses: handed-out ranges lie
 // inside one chunk, never overlap, are aligned; released ranges merge back so
 // that an emptied arena hands every chunk back whole; chunks that happen to be
-// adjacent in the address space are never merged.  Exit 0 and "OK" on success.
+// adjacent in the address space are never merged; chunks handed back while
+// other chunks still hold ranges contain no live range and are never handed
+// out again.  Exit 0 and "OK" on success.
 #include <cstdio>
 #include <map>
 #include <random>
@@ -63,6 +65,21 @@ int main() {
       size_t used = 0;
       for (auto& kv : live) used += Arena::round(kv.second);
       CHECK(used == a.bytesUsed());
+    }
+  }
+  {  // chunks handed back while others hold live ranges: only empty ones go
+    auto chunksBefore = a.chunks();
+    auto freed = a.takeFreeChunks();
+    for (auto& f : freed)
+      for (auto& kv : live) CHECK(!(kv.first >= f.first && kv.first < f.first + f.second));
+    CHECK(a.chunks().size() + freed.size() == chunksBefore.size());
+    for (int t = 0; t < 2000; ++t) {  // later ranges never fall in a returned chunk
+      const uint64_t p = a.alloc((size_t)1 << (18 + rng() % 10));
+      CHECK(p != 0);
+      for (auto& f : freed) CHECK(!(p >= f.first && p < f.first + f.second));
+      live[p] = 0;
+      CHECK(a.release(p));
+      live.erase(p);
     }
   }
   CHECK(!a.release(12345));  // not an address the arena handed out
