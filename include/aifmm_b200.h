@@ -292,8 +292,16 @@ int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const vo
 int aifmm_profile_ops(int on);
 int aifmm_profile_ops_read(char* buf, int cap);
 /* Number of tcgen05 GEMM tiles whose bounded pipeline wait ran out (their
- * output was left unwritten); 0 in a healthy run. */
+ * output was left unwritten); 0 in a healthy run.  The factorization and the
+ * GEMM entry points compare this count before and after their work and
+ * return AIFMM_ETIMEOUT when it grew. */
 int aifmm_tc5_timeouts(long* n);
+/* Test of the bounded waits (no counterpart in the reference): with on = 1,
+ * the tensor-core GEMMs of this context first wait, for at most 1 ms, on a
+ * device flag that nothing sets, so every tile gives up, writes nothing and
+ * the call returns AIFMM_ETIMEOUT with the context still usable; on = 0
+ * restores normal operation. */
+int aifmm_debug_gemm_hold(aifmm_ctx* ctx, int on);
 /* Number of CUDA kernels this library has launched in the process. */
 int aifmm_launch_count(long* n);
 /* Switch per-launch CUDA-event timing of the grouped complex GEMM on (1) or

@@ -56,6 +56,7 @@ SIGNATURES = {
     "aifmm_solver_rewind": (_i, [_p]),
     "aifmm_launch_count": (_i, [C.POINTER(C.c_long)]),
     "aifmm_tc5_timeouts": (_i, [C.POINTER(C.c_long)]),
+    "aifmm_debug_gemm_hold": (_i, [_p, _i]),
     "aifmm_profile_ops": (_i, [_i]),
     "aifmm_profile_ops_read": (_i, [C.c_char_p, _i]),
     "aifmm_aca": (_i, [_p, _ip, _i, _ip, _i, _d, _ip, _ip, C.POINTER(_i), _dp, _dp]),

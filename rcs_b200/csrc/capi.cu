@@ -5,6 +5,7 @@
 #include <cmath>
 #include <cstring>
 #include <mutex>
+#include <set>
 
 #include "capi_guard.cuh"
 #include "context.cuh"
@@ -20,6 +21,15 @@ void count_launch(long n) { g_launches += n; }
 long launch_count() { return g_launches.load(); }
 
 static std::mutex g_ctx_mu;
+
+void smem_attr_once(const void* kernel, int device, int bytes) {
+  static std::mutex mu;
+  static std::set<std::pair<const void*, int>> done;
+  std::lock_guard<std::mutex> l(mu);
+  if (done.count({kernel, device})) return;
+  AIFMM_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  done.insert({kernel, device});
+}
 
 void ctx_retain(aifmm_ctx* c) {
   std::lock_guard<std::mutex> l(g_ctx_mu);
@@ -39,6 +49,7 @@ void ctx_release(aifmm_ctx* c) {
   for (int i = 0; i < aifmm_ctx::kRingChunks; ++i)
     if (c->ringEvent[i]) cudaEventDestroy(c->ringEvent[i]);
   if (c->ring) cudaFreeHost(c->ring);
+  if (c->holdFlag) cudaFree(c->holdFlag);
   if (c->arena) {
     for (auto& ch : c->arena->chunks()) cudaFreeAsync((void*)ch.first, c->stream);
     c->arena.reset();
@@ -171,7 +182,19 @@ int aifmm_profile_ops_read(char* buf, int cap) {
 int aifmm_tc5_timeouts(long* n) {
   API_BEGIN
   AIFMM_REQUIRE(n, AIFMM_EINVAL, "NULL argument");
-  *n = zgemm_tc5_timeouts() + zgemm_tc5p_timeouts();
+  *n = tc_timeouts();
+  API_END
+}
+
+int aifmm_debug_gemm_hold(aifmm_ctx* ctx, int on) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx, AIFMM_EINVAL, "ctx is NULL");
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  if (on && !ctx->holdFlag) {
+    AIFMM_CUDA(cudaMalloc((void**)&ctx->holdFlag, sizeof(int)));
+    AIFMM_CUDA(cudaMemset(ctx->holdFlag, 0, sizeof(int)));
+  }
+  ctx->gemmHold = on != 0;
   API_END
 }
 

@@ -19,6 +19,10 @@ struct Error : std::runtime_error {
 };
 
 void set_last_error(const std::string& msg);
+// cudaFuncSetAttribute(kernel, MaxDynamicSharedMemorySize, bytes) once per
+// (kernel, device), safe to call from several host threads; the device must
+// be current.
+void smem_attr_once(const void* kernel, int device, int bytes);
 // Number of kernels this library has launched (all contexts, process-wide).
 void count_launch(long n = 1);
 long launch_count();

@@ -160,6 +160,7 @@ static void zgemm_checked(aifmm_ctx* ctx, int precision, int opA, int opB, int m
   GemmProblem g{A, B, C, m, n, k, lda, ldb, ldc, opA, opB, zmk(alpha[0], alpha[1]), zmk(beta[0], beta[1])};
   const int saved = ctx->gemmPrecision;
   ctx->gemmPrecision = precision;
+  const long t0 = precision >= 2 ? tc_timeouts() : 0;
   try {
     zgemm_grouped(ctx, {g});
   } catch (...) {
@@ -167,6 +168,10 @@ static void zgemm_checked(aifmm_ctx* ctx, int precision, int opA, int opB, int m
     throw;
   }
   ctx->gemmPrecision = saved;
+  if (precision >= 2) {  // a tile that gave up on a bounded wait left C unwritten
+    AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+    tc_check(t0, "zgemm");
+  }
 }
 
 static void zgemm_args(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double* alpha,

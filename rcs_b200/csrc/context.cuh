@@ -34,6 +34,12 @@ struct aifmm_ctx {
   cudaEvent_t ringEvent[kRingChunks] = {};
   long ringChunkLap[kRingChunks] = {};  // 0: never used
   bool closed = false;
+  // Wait test of the tensor-core GEMMs (aifmm_debug_gemm_hold): when set, their
+  // issuing thread first waits, bounded by 1 ms, on `holdFlag`, a device int
+  // that stays zero, so every tile times out and the call reports
+  // AIFMM_ETIMEOUT.
+  bool gemmHold = false;
+  int* holdFlag = nullptr;
   // Sub-allocator for the blocks of 256 KB and more (arena.cuh); its chunks
   // come from `pool`.  Created with the context.
   std::mutex arenaMu;

@@ -558,6 +558,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
   a.ngroups = (int)gs.size();
   a.probs = nullptr;
   a.groups = nullptr;
+  tc_wait_args(ctx, a);
   DevBuf dp, dg;
   const bool inl = gs.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
   if (inl) {
@@ -583,15 +584,8 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     if (inl) zgemm_tf32x3_kernel<true><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
     else zgemm_tf32x3_kernel<false><<<(unsigned)tiles, 256, 0, ctx->stream>>>(a);
   } else {
-    static bool attr[256] = {};
-    AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
-    if (!attr[ctx->device]) {
-      AIFMM_CUDA(cudaFuncSetAttribute(zgemm_grouped_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(GemmSmem)));
-      AIFMM_CUDA(cudaFuncSetAttribute(zgemm_grouped_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)sizeof(GemmSmem)));
-      attr[ctx->device] = true;
-    }
+    smem_attr_once((const void*)zgemm_grouped_kernel<true>, ctx->device, (int)sizeof(GemmSmem));
+    smem_attr_once((const void*)zgemm_grouped_kernel<false>, ctx->device, (int)sizeof(GemmSmem));
     if (inl) zgemm_grouped_kernel<true><<<(unsigned)tiles, 256, sizeof(GemmSmem), ctx->stream>>>(a);
     else zgemm_grouped_kernel<false><<<(unsigned)tiles, 256, sizeof(GemmSmem), ctx->stream>>>(a);
   }
@@ -940,13 +934,7 @@ void zgetrs(aifmm_ctx* ctx, const zd* LU, int n, int lda, const int* piv, zd* B,
   if (n <= 0 || nrhs <= 0) return;
   const size_t smem = sizeof(zd) * (size_t)n * nrhs;
   if (nrhs <= 16 && smem <= GS_SMEM_MAX) {
-    static bool attr[256] = {};  // the attribute is set once per device
-    AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
-    if (!attr[ctx->device]) {
-      AIFMM_CUDA(cudaFuncSetAttribute(zgetrs_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)GS_SMEM_MAX));
-      attr[ctx->device] = true;
-    }
+    smem_attr_once((const void*)zgetrs_smem_kernel, ctx->device, (int)GS_SMEM_MAX);
     zgetrs_smem_kernel<<<1, GS_NT, smem, ctx->stream>>>(LU, n, lda, piv, B, nrhs, ldb);
     AIFMM_LAUNCHED();
     return;

@@ -38,6 +38,12 @@ struct GemmArgs {
   int ngroups;
   const GemmProblem* probs;
   const GemmGroup* groups;
+  // tensor-core kernels: limit of each bounded pipeline wait (ns), and an
+  // optional device flag that the issuing thread waits on before its first
+  // copy (null in normal use; the library's wait test points it at a flag
+  // that nothing sets, so that the wait runs out)
+  unsigned long long waitNs;
+  const int* hold;
   GemmProblem ip[GEMM_INLINE];
   GemmGroup ig[GEMM_INLINE];
 };
@@ -47,6 +53,12 @@ struct GemmArgs {
 void zgemm_tc5_launch(aifmm_ctx* ctx, const GemmArgs& a, bool inl, long tiles);
 // Number of tcgen05 pipeline waits that ran out (each leaves its tile unwritten).
 long zgemm_tc5_timeouts();
+// Sum of both tensor-core GEMMs' timeout counters, and a check that throws
+// AIFMM_ETIMEOUT when it grew past `before` (call after the stream drained).
+long tc_timeouts();
+void tc_check(long before, const char* what);
+// Fills the wait limit and hold flag of a tensor-core launch from the context.
+void tc_wait_args(aifmm_ctx* ctx, GemmArgs& a);
 // The tensor-core GEMM over pre-tiled operand planes (zgemm_tc5p.cu): the
 // operands of every problem are first converted once into split-TF32 planes
 // laid out tile by tile, then each CTA streams its tiles with bulk copies.

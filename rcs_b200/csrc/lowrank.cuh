@@ -38,7 +38,7 @@ struct RRQRProblem {
   zd* H;             // m x (min(m,n)+1) reflector storage
   double* nsq;       // n
   int* perm;         // n
-  zd* Q;             // out: m x rank (ld = m), space for m x (min(m,n)+1)
+  zd* Q;             // out: m x rank (ld = m); at most min(m,n) columns are written
   int* rank;         // out
   double* maxPivot;  // out
   int* istate;       // split pipeline only: 8 ints of scratch

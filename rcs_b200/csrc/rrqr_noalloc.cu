@@ -8,16 +8,22 @@
 // permutation) lives in the fixed-size device array below, which every GPU
 // that loads this library keeps until the process exits.
 //
-// Set-up: the first call on a device, with that device current, looks up the
-// array's device address with cudaGetSymbolAddress (the name of a
-// __device__ array is only a host-side stand-in, not a device address) and
-// caches it.  Make that first call before any stream capture.
+// Set-up: the first call in a CUDA context (normally a device's primary
+// context), with that device current, looks up the array's device address
+// with cudaGetSymbolAddress (the name of a __device__ array is only a
+// host-side stand-in, not a device address) and caches it for that context.
+// Make that first call before any stream capture.  A context created later
+// (after cudaDeviceReset, or another context made current) gets its own
+// lookup on its first call.
 //
 // All calls share the one array: calls whose work overlaps on the GPU (two
 // streams, or two host threads) race and corrupt each other.  Serialise them,
 // e.g. on one stream.
+#include <cuda.h>
+
 #include <algorithm>
 #include <cmath>
+#include <map>
 #include <mutex>
 
 #include "lowrank.cuh"
@@ -33,10 +39,31 @@ constexpr int kRRQRThreads = 1024;
 constexpr size_t kNoAllocScratchBytes = (size_t)32 << 20;
 static __device__ __align__(256) unsigned char g_rrqr_scratch[kNoAllocScratchBytes];
 
+// The descriptor of the problem sits in the array's first KiB.
+static_assert(sizeof(RRQRProblem) <= 1024, "the RRQR descriptor must fit the scratch array's first KiB");
+
 static std::mutex g_scratch_mu;
-static void* g_scratch_addr[128] = {nullptr};
+static std::map<CUcontext, void*> g_scratch_addr;  // per CUDA context
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+// The calling thread's current CUDA context, through the driver entry point
+// that the runtime hands out (the library does not link the driver library).
+static CUcontext current_context() {
+  using Fn = CUresult (*)(CUcontext*);
+  static Fn fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<Fn>(p);
+  });
+  CUcontext c = nullptr;
+  if (!fn || fn(&c) != CUDA_SUCCESS) return nullptr;
+  return c;
+}
 
 __global__ void rrqr_noalloc_setup_kernel(RRQRProblem P, RRQRProblem* dst, const zd* A) {
   if (blockIdx.x == 0 && threadIdx.x == 0) *dst = P;
@@ -66,18 +93,24 @@ extern "C" int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partit
     AIFMM_REQUIRE(need <= kNoAllocScratchBytes, AIFMM_EOVERFLOW,
                   "problem needs " + std::to_string(need) + " bytes of scratch; the fixed scratch array holds " +
                       std::to_string(kNoAllocScratchBytes));
-    int dev = 0;
-    AIFMM_CUDA(cudaGetDevice(&dev));
-    AIFMM_REQUIRE(dev >= 0 && dev < 128, AIFMM_EINVAL, "device index out of range");
+    CUcontext cu = current_context();
+    if (!cu) {
+      int dev = 0;  // nothing current yet: cudaSetDevice makes the device's primary context current
+      AIFMM_CUDA(cudaGetDevice(&dev));
+      AIFMM_CUDA(cudaSetDevice(dev));
+      cu = current_context();
+      AIFMM_REQUIRE(cu, AIFMM_ECUDA, "no current CUDA context");
+    }
     void* base = nullptr;
     {
       std::lock_guard<std::mutex> l(g_scratch_mu);
-      if (!g_scratch_addr[dev]) {
+      auto it = g_scratch_addr.find(cu);
+      if (it == g_scratch_addr.end()) {
         void* p = nullptr;
-        AIFMM_CUDA(cudaGetSymbolAddress(&p, g_rrqr_scratch));  // with this device current
-        g_scratch_addr[dev] = p;
+        AIFMM_CUDA(cudaGetSymbolAddress(&p, g_rrqr_scratch));  // in this context, with this device current
+        it = g_scratch_addr.emplace(cu, p).first;
       }
-      base = g_scratch_addr[dev];
+      base = it->second;
     }
     unsigned char* b = static_cast<unsigned char*>(base);
     RRQRProblem P;

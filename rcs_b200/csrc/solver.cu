@@ -1190,6 +1190,7 @@ void Solver::eliminateZ(int j, int k) {
 void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   const double t0 = wall();
   AIFMM_CUDA(cudaSetDevice(ctx->device));
+  const long tc0 = prm.precision >= 2 ? tc_timeouts() : 0;
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
   stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
@@ -1230,6 +1231,8 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
     }
   }
   ops.sync();
+  // a tensor-core tile that gave up on a bounded wait left its Schur block unwritten
+  if (prm.precision >= 2) tc_check(tc0, "factorize");
   factored = true;
   stats.t_factor = wall() - t0;
 }

@@ -84,7 +84,8 @@ __device__ __forceinline__ unsigned long long c5_now() {
 
 // Wait for the completion of the barrier phase with the given parity; false
 // if that takes longer than C5_WAIT_NS.
-__device__ __forceinline__ bool c5_wait(unsigned long long* bar, uint32_t parity) {
+__device__ __forceinline__ bool c5_wait(unsigned long long* bar, uint32_t parity,
+                                        unsigned long long limit = C5_WAIT_NS) {
   const uint32_t a = c5_smem_addr(bar);
   const unsigned long long t0 = c5_now();
   while (true) {
@@ -96,8 +97,15 @@ __device__ __forceinline__ bool c5_wait(unsigned long long* bar, uint32_t parity
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if (c5_now() - t0 > C5_WAIT_NS) return false;
+    if (c5_now() - t0 > limit) return false;
   }
+}
+// Bounded wait until *flag != 0 (the wait test's hold flag).
+__device__ __forceinline__ bool c5_hold(const int* flag, unsigned long long limit) {
+  const unsigned long long t0 = c5_now();
+  while (*(const volatile int*)flag == 0)
+    if (c5_now() - t0 > limit) return false;
+  return true;
 }
 
 __device__ __forceinline__ uint32_t c5_tf32(float x) {
@@ -174,6 +182,11 @@ __global__ void __launch_bounds__(C5_THREADS, 2) zgemm_tc5_kernel(const __grid_c
   uint32_t phase[2] = {0, 0};
   int it = 0;
   bool ok = true, crInit = false, ciInit = false;
+  if (a.hold) {  // the wait test's hold: before any MMA, so nothing is in flight if it runs out
+    bool mine = true;
+    if (tid == 0) mine = c5_hold(a.hold, a.waitNs);
+    ok = __syncthreads_and(mine);
+  }
   for (int q = 0; q < g.nchain && ok; ++q) {
     const GemmProblem& P = probs[g.head + q];
     if (P.k <= 0) continue;
@@ -197,7 +210,7 @@ __global__ void __launch_bounds__(C5_THREADS, 2) zgemm_tc5_kernel(const __grid_c
       const int s = it & 1;
       if (it >= 2) {  // the MMAs that read this stage two slices ago must be done
         bool mine = true;
-        if (tid == 0) mine = c5_wait(&S.bar[s], phase[s]);
+        if (tid == 0) mine = c5_wait(&S.bar[s], phase[s], a.waitNs);
         ok = __syncthreads_and(mine);
         phase[s] ^= 1;
         if (!ok) break;
@@ -256,7 +269,7 @@ __global__ void __launch_bounds__(C5_THREADS, 2) zgemm_tc5_kernel(const __grid_c
   if (ok && it > 0) {  // the last commit covers every MMA issued before it
     const int s = (it - 1) & 1;
     bool mine = true;
-    if (tid == 0) mine = c5_wait(&S.bar[s], phase[s]);
+    if (tid == 0) mine = c5_wait(&S.bar[s], phase[s], a.waitNs);
     ok = __syncthreads_and(mine);
   }
   asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
@@ -312,13 +325,8 @@ __global__ void __launch_bounds__(C5_THREADS, 2) zgemm_tc5_kernel(const __grid_c
 
 void zgemm_tc5_launch(aifmm_ctx* ctx, const GemmArgs& a, bool inl, long tiles) {
   const size_t smem = sizeof(C5Smem) + 1024;
-  static bool attr[256] = {};
-  AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
-  if (!attr[ctx->device]) {
-    AIFMM_CUDA(cudaFuncSetAttribute(zgemm_tc5_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    AIFMM_CUDA(cudaFuncSetAttribute(zgemm_tc5_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr[ctx->device] = true;
-  }
+  smem_attr_once((const void*)zgemm_tc5_kernel<true>, ctx->device, (int)smem);
+  smem_attr_once((const void*)zgemm_tc5_kernel<false>, ctx->device, (int)smem);
   if (inl) zgemm_tc5_kernel<true><<<(unsigned)tiles, C5_THREADS, smem, ctx->stream>>>(a);
   else zgemm_tc5_kernel<false><<<(unsigned)tiles, C5_THREADS, smem, ctx->stream>>>(a);
   AIFMM_LAUNCHED();

@@ -67,7 +67,8 @@ __device__ __forceinline__ unsigned long long p5_now() {
   asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
   return t;
 }
-__device__ __forceinline__ bool p5_wait(unsigned long long* bar, uint32_t parity) {
+__device__ __forceinline__ bool p5_wait(unsigned long long* bar, uint32_t parity,
+                                        unsigned long long limit = P5_WAIT_NS) {
   const uint32_t a = p5_smem(bar);
   const unsigned long long t0 = p5_now();
   while (true) {
@@ -79,8 +80,15 @@ __device__ __forceinline__ bool p5_wait(unsigned long long* bar, uint32_t parity
         : "r"(a), "r"(parity)
         : "memory");
     if (done) return true;
-    if (p5_now() - t0 > P5_WAIT_NS) return false;
+    if (p5_now() - t0 > limit) return false;
   }
+}
+// Bounded wait until *flag != 0 (the wait test's hold flag).
+__device__ __forceinline__ bool p5_hold(const int* flag, unsigned long long limit) {
+  const unsigned long long t0 = p5_now();
+  while (*(const volatile int*)flag == 0)
+    if (p5_now() - t0 > limit) return false;
+  return true;
 }
 // Bulk copies of slice `it` into ring slot s, completing on full[s].
 __device__ __forceinline__ void p5_load(P5Smem& S, int s, const uint32_t* ga, const uint32_t* gb) {
@@ -208,20 +216,25 @@ __global__ void __launch_bounds__(P5_THREADS, 1) zgemm_tc5p_kernel(const __grid_
       pb = P.pb + ((size_t)tn * nks + ks) * (P5_B_BYTES / 4);
     };
     uint32_t fph[P5_STAGES] = {0, 0, 0, 0}, eph[P5_STAGES] = {0, 0, 0, 0};
-    bool ok = true;
-    const int pre = min(total, P5_STAGES);
+    bool loaded[P5_STAGES] = {false, false, false, false};  // a copy whose full phase is not consumed yet
+    const unsigned long long lim = a.waitNs;
+    // the wait test's hold comes before any copy, so nothing is in flight if it runs out
+    bool ok = !(a.hold && !p5_hold(a.hold, lim));
+    const int pre = ok ? min(total, P5_STAGES) : 0;
     for (int it = 0; it < pre; ++it) {
       const uint32_t *pa, *pb;
       src(it, pa, pb);
       p5_load(S, it, pa, pb);
+      loaded[it] = true;
     }
     constexpr uint32_t ip = p5_idesc(false), in = p5_idesc(true);
     const uint32_t dr = tmem, di = tmem + P5_N;
-    int issuedLoads = pre;
+    int issuedLoads = pre, lastCommit = -1;
     for (int it = 0; it < total && ok; ++it) {
       const int s = it % P5_STAGES;
-      if (!p5_wait(&S.full[s], fph[s])) { ok = false; break; }
+      if (!p5_wait(&S.full[s], fph[s], lim)) { ok = false; break; }
       fph[s] ^= 1;
+      loaded[s] = false;
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       P5Stage& st = S.st[s];
 #pragma unroll
@@ -246,26 +259,34 @@ __global__ void __launch_bounds__(P5_THREADS, 1) zgemm_tc5p_kernel(const __grid_
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                        p5_smem(&S.empty[s]))
                    : "memory");
+      lastCommit = it;
       // refill the previous slice's slot once its MMAs are done
       if (it >= 1 && issuedLoads < total) {
         const int sp = (it - 1) % P5_STAGES;
-        if (!p5_wait(&S.empty[sp], eph[sp])) { ok = false; break; }
+        if (!p5_wait(&S.empty[sp], eph[sp], lim)) { ok = false; break; }
         eph[sp] ^= 1;
         const uint32_t *pa, *pb;
         src(issuedLoads, pa, pb);
         p5_load(S, sp, pa, pb);
+        loaded[sp] = true;
         ++issuedLoads;
       }
     }
     if (ok) {  // the last commit covers every MMA
       const int sl = (total - 1) % P5_STAGES;
       // slots whose empty phase was already consumed by a refill wait are not waited again
-      ok = p5_wait(&S.empty[sl], eph[sl]);
+      ok = p5_wait(&S.empty[sl], eph[sl], lim);
+    } else {
+      // drain before the tile is abandoned: the MMAs of the last commit (they
+      // read shared memory and write tensor memory) and every copy in flight,
+      // each wait bounded by the normal limit
+      if (lastCommit >= 0) p5_wait(&S.empty[lastCommit % P5_STAGES], eph[lastCommit % P5_STAGES]);
+      for (int s = 0; s < P5_STAGES; ++s)
+        if (loaded[s]) p5_wait(&S.full[s], fph[s]);
     }
     if (!ok) {
       atomicAdd(&g_p5_timeouts, 1ull);
       S.ok = 0;
-      for (int s = 0; s < P5_STAGES; ++s) p5_wait(&S.full[s], fph[s]);  // bounded: copies in flight
     }
   }
   asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -394,6 +415,7 @@ static void p5_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
   a.ngroups = (int)groups.size();
   a.probs = nullptr;
   a.groups = nullptr;
+  tc_wait_args(ctx, a);
   DevBuf dp, dg;
   const bool inl = groups.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
   if (inl) {
@@ -406,13 +428,8 @@ static void p5_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
     a.groups = dg.as<GemmGroup>();
   }
   const size_t smem = sizeof(P5Smem) + 1024;
-  static bool attr[256] = {};
-  AIFMM_REQUIRE(ctx->device >= 0 && ctx->device < 256, AIFMM_EINVAL, "device index out of range");
-  if (!attr[ctx->device]) {
-    AIFMM_CUDA(cudaFuncSetAttribute(zgemm_tc5p_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    AIFMM_CUDA(cudaFuncSetAttribute(zgemm_tc5p_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    attr[ctx->device] = true;
-  }
+  smem_attr_once((const void*)zgemm_tc5p_kernel<true>, ctx->device, (int)smem);
+  smem_attr_once((const void*)zgemm_tc5p_kernel<false>, ctx->device, (int)smem);
   if (inl) zgemm_tc5p_kernel<true><<<(unsigned)tiles, P5_THREADS, smem, ctx->stream>>>(a);
   else zgemm_tc5p_kernel<false><<<(unsigned)tiles, P5_THREADS, smem, ctx->stream>>>(a);
   AIFMM_LAUNCHED();
@@ -454,6 +471,21 @@ long zgemm_tc5p_timeouts() {
   unsigned long long v = 0;
   AIFMM_CUDA(cudaMemcpyFromSymbol(&v, g_p5_timeouts, sizeof(v)));
   return (long)v;
+}
+
+long tc_timeouts() { return zgemm_tc5_timeouts() + zgemm_tc5p_timeouts(); }
+
+void tc_check(long before, const char* what) {
+  const long now = tc_timeouts();
+  if (now > before)
+    throw Error(AIFMM_ETIMEOUT, std::string(what) + ": " + std::to_string(now - before) +
+                                    " tensor-core GEMM tile(s) gave up on a bounded pipeline wait; their output "
+                                    "blocks are not written");
+}
+
+void tc_wait_args(aifmm_ctx* ctx, GemmArgs& a) {
+  a.hold = ctx->gemmHold ? ctx->holdFlag : nullptr;
+  a.waitNs = ctx->gemmHold ? 1000000ull : P5_WAIT_NS;
 }
 
 }  // namespace aifmm

@@ -123,9 +123,41 @@ def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
     ref = alpha * ((A.conj().T if opA else A) @ (B.conj().T if opB else B)) + beta * C0
     scale = abs(alpha) * np.linalg.norm(A) * np.linalg.norm(B) + abs(beta) * np.linalg.norm(C0)
     assert np.linalg.norm(C - ref) <= bound * scale
+    if precision >= 1 and k >= 16:  # split TF32 with FP32 accumulation, not an FP64 product
+        assert np.linalg.norm(C - ref) >= 1e-12 * scale
     if precision >= 2:  # no tcgen05 pipeline wait ran out
         import ctypes as Cc
         from rcs_b200 import _lib
         n_to = Cc.c_long()
         _lib.check(_lib.lib().aifmm_tc5_timeouts(Cc.byref(n_to)))
         assert n_to.value == 0
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("precision", [2, 3])
+def test_tensor_core_wait_timeout_is_an_error(precision):
+    """A tensor-core GEMM whose bounded wait runs out returns AIFMM_ETIMEOUT
+    (not a silently unwritten C), and the context stays usable: the wait test
+    holds every tile on a device flag that nothing sets, for at most 1 ms."""
+    import ctypes as Cc
+    from rcs_b200 import _lib
+    from rcs_b200.kernel import Context
+    ctx = Context(0)
+    rng = np.random.default_rng(5)
+    A = rng.standard_normal((200, 96)) + 1j * rng.standard_normal((200, 96))
+    B = rng.standard_normal((96, 70)) + 1j * rng.standard_normal((96, 70))
+    n0 = Cc.c_long()
+    _lib.check(_lib.lib().aifmm_tc5_timeouts(Cc.byref(n0)))
+    _lib.check(_lib.lib().aifmm_debug_gemm_hold(ctx.h, 1))
+    try:
+        with pytest.raises(RuntimeError) as e:
+            lowrank.zgemm(A, B, precision=precision, ctx=ctx)
+        assert "gave up" in str(e.value)
+    finally:
+        _lib.check(_lib.lib().aifmm_debug_gemm_hold(ctx.h, 0))
+    n1 = Cc.c_long()
+    _lib.check(_lib.lib().aifmm_tc5_timeouts(Cc.byref(n1)))
+    assert n1.value - n0.value == 2 * 2  # 2 row tiles x 2 column tiles, each gave up once
+    C = lowrank.zgemm(A, B, precision=precision, ctx=ctx)  # the same context afterwards
+    assert np.linalg.norm(C - A @ B) <= 2e-6 * np.linalg.norm(A) * np.linalg.norm(B)
+    ctx.close()

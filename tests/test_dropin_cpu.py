@@ -13,7 +13,9 @@ from rcs_b200 import dropin
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 CPP = os.path.join(ROOT, "tests", "cpp")
-REFERENCE_DRIVER = "/root/reference/test/sphere.cpp"
+# The reference source tree (vaishna77/RCS), when it is present on this machine.
+REFERENCE_ROOT = os.environ.get("AIFMM_REFERENCE_ROOT", "")
+REFERENCE_DRIVER = os.path.join(REFERENCE_ROOT, "test", "sphere.cpp") if REFERENCE_ROOT else ""
 
 pytestmark = pytest.mark.skipif(shutil.which("g++") is None, reason="g++ not available")
 
