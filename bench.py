@@ -35,24 +35,22 @@ METRIC = "factor+solve s at rel. residual 1e-6: mixed/batched/learned vs plain F
 # ACA tolerance of the FP64 H^2 forward operator that GMRES iterates on; gmres:
 # target relative residual (None = direct solve only, the reference's path).
 CONFIGS = {
-    "c1": dict(sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0, op_tol=None,
+    "c1": dict(N=1920, sub=3, radius=0.15, freq=1.0e9, leaf=64, tol_pow=8, fillin_tol=10, nrhs=1, levels=0, op_tol=None,
                gmres=None, precision=0,
                desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10, "
                     "direct solve"),
-    "c3": dict(sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
+    "c3": dict(N=122880, sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
                gmres=1e-6, precision=3,
                desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
                     "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs over pre-tiled "
                     "planes) as the preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
-    "c3s": dict(sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
+    "c3s": dict(N=30720, sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
                 gmres=1e-6, precision=3,
                 desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
                      "8 plane waves, FGMRES(30) to 1e-6 (c3 shape at 1/4 size)"),
 }
-# CPU sample for the reference arm and cpu_baseline: the c3 sphere and
-# frequency on the 1,280-triangle mesh (N=1,920) with c3's tree depth (3
-# levels) and tolerances; about 25 s of oracle factor+solve on 8 cores.
-CPU_SAMPLE = dict(sub=3, radius=0.15, freq=4.0e9, leaf=8, tol_pow=5, fillin_tol=7, nrhs=1, levels=3)
+# CPU baseline (reference arm and cpu_baseline): pair updates per timed sample.
+CPU_PAIRS_PER_SAMPLE = 16
 
 
 def plane_waves(n: int, seed: int = 4):
@@ -195,70 +193,140 @@ def zgemm_peak_tflops() -> float:
     return 8.0 * n ** 3 / best / 1e12
 
 
-def cpu_sample_seconds(threads: int):
-    """Oracle (the reference's CPU algorithm restated) factor + direct solve on
-    the CPU sample; returns seconds and the sample's unknown count."""
-    import oracle
-    from rcs_b200 import mesh as M
-    oracle.set_threads(threads)
-    m = M.icosphere(CPU_SAMPLE["sub"], CPU_SAMPLE["radius"])
-    O = oracle.EFIE(m, CPU_SAMPLE["freq"])
-    b = O.rhs_plane((0, 0, -1), (1, 0, 0))
-    S = oracle.AIFMM(O, leaf_size=CPU_SAMPLE["leaf"], tol_pow=CPU_SAMPLE["tol_pow"],
-                     fillin_tol=CPU_SAMPLE["fillin_tol"], n_levels=CPU_SAMPLE["levels"])
-    t0 = time.perf_counter()
-    S.factorize()
-    S.solve(b)
-    return time.perf_counter() - t0
+class CPUBaseline:
+    """The reference's CPU algorithm (the oracle, a C++ restatement; the
+    reference itself needs Eigen 3, absent here) on the benchmark's own tree.
+
+    The full factorization of the 122,880-unknown sphere takes hours on the
+    host, so one sample times a bounded piece of it: for one leaf box k of the
+    workload's tree, the LU of its near-field block and up to
+    CPU_PAIRS_PER_SAMPLE of the near-field Schur updates that the
+    reference's eliminate_x performs for it (P2P[nn][pp] -= P2P[nn][k]
+    lu.solve(P2P[k][pp]) for neighbours nn, pp not yet eliminated, the solve
+    recomputed per pair as the reference does), at the workload's block
+    sizes.  The extrapolation multiplies the measured seconds per complex
+    multiply-add by the multiply-adds of every such update of the leaf level,
+    counted from the tree's box sizes and neighbour lists in elimination
+    order, plus three LUs per leaf box (the factorization's and the two of
+    the reference's solve).  It leaves out the rank-sized updates, eliminate_z,
+    the recompressions, the non-leaf level and the assembly, so it is a LOWER
+    BOUND on the reference's factor+solve time."""
+
+    def __init__(self, cfg):
+        import oracle
+        from rcs_b200 import mesh as M
+        self.oracle = oracle
+        self.cfg = cfg
+        m = M.icosphere(cfg["sub"], cfg["radius"])
+        self.K = oracle.EFIE(m, cfg["freq"]) if cfg.get("kind", "efie") == "efie" else oracle.Electrostatics(m)
+        self.n_levels, self.leaves, self.nbs = oracle.tree_shape(self.K, cfg["leaf"], cfg["levels"])
+        sizes = np.array([len(v) for v in self.leaves], dtype=np.float64)
+        self.lu_macs = 0.0
+        self.pair_macs = 0.0
+        self.n_pairs = 0
+        self.cands = []
+        for k, mk in enumerate(sizes):
+            if mk == 0:
+                continue
+            self.lu_macs += 3 * mk ** 3 / 3.0
+            live = [nn for nn in self.nbs[k] if nn != k and nn > k and sizes[nn] > 0]
+            for nn in live:
+                for pp in live:
+                    self.pair_macs += mk * mk * sizes[pp] + sizes[nn] * mk * sizes[pp]
+                    self.n_pairs += 1
+            if live:
+                self.cands.append(k)
+        self.order = np.random.default_rng(20261204).permutation(len(self.cands))
+        self.samples = []
+
+    def sample(self, i: int, threads: int):
+        """Sample i: (seconds, lu seconds, pair seconds, lu macs, pair macs)."""
+        k = self.cands[self.order[i % len(self.order)]]
+        sizes = [len(v) for v in self.leaves]
+        live = [nn for nn in self.nbs[k] if nn != k and nn > k and sizes[nn] > 0]
+        pairs = [(a, b) for a in range(len(live)) for b in range(len(live))]
+        rng = np.random.default_rng(i)
+        if len(pairs) > CPU_PAIRS_PER_SAMPLE:
+            pairs = [pairs[q] for q in sorted(rng.choice(len(pairs), CPU_PAIRS_PER_SAMPLE, replace=False))]
+        s_lu, s_pairs, m_lu, m_pairs = self.oracle.schur_sample(self.K, self.leaves[k],
+                                                               [self.leaves[nn] for nn in live], pairs, threads)
+        r = dict(box=int(k), m=sizes[k], pairs=len(pairs), s_lu=s_lu, s_pairs=s_pairs, m_lu=m_lu, m_pairs=m_pairs)
+        return s_lu + s_pairs, r
+
+    @staticmethod
+    def extrapolate(recs, lu_macs, pair_macs) -> float:
+        s_lu = sum(r["s_lu"] for r in recs)
+        s_p = sum(r["s_pairs"] for r in recs)
+        m_lu = sum(r["m_lu"] for r in recs)
+        m_p = sum(r["m_pairs"] for r in recs)
+        return lu_macs * s_lu / m_lu + pair_macs * s_p / m_p
+
+    def describe(self, recs, threads: int) -> str:
+        return (f"oracle (C++ restatement of the reference) on the workload's own tree ({self.n_levels} levels, "
+                f"{len(self.cands)} leaf boxes with near-field updates, {self.n_pairs} updates in elimination "
+                f"order): {len(recs)} timed samples on {threads} thread(s), each one leaf box's near-field LU "
+                f"and up to {CPU_PAIRS_PER_SAMPLE} of its pair updates at the workload's block sizes "
+                f"({sum(r['s_lu'] + r['s_pairs'] for r in recs):.1f} s timed); extrapolated by complex "
+                f"multiply-adds to every leaf near-field update and three LUs per leaf box "
+                f"({(self.lu_macs + self.pair_macs) / 1e12:.2f} T multiply-adds).  A lower bound: rank-sized "
+                f"updates, eliminate_z, recompressions, the non-leaf level and assembly are not counted")
 
 
-def factor_flops(c, ctx) -> float:
-    """Algorithmic factorization flops of a config, counted by the GPU run of
-    the same algorithm (the oracle cannot run the full workload in minutes)."""
-    from rcs_b200 import mesh as M
-    from rcs_b200.kernel import EFIEMatrix
-    from rcs_b200.solver import AIFMM
-    K = EFIEMatrix(M.icosphere(c["sub"], c["radius"]), c["freq"], ctx=ctx)
-    S = AIFMM(K, leaf_size=c["leaf"], tol_pow=c["tol_pow"], fillin_tol=c["fillin_tol"], n_levels=c["levels"])
-    S.factorize()
-    f = S.info()["flops_factor"]
-    S.close()
-    K.close()
-    return f
+def peaks():
+    """MEASURED_PEAKS.json (driver-written, measured on this pool's B200s) or
+    the recorded fallback figures of this pool."""
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return {"hbm_gbs": float(d["hbm_gbs"]), "bf16_tflops": float(d["bf16_tflops"]),
+                "bf16_tflops_sustained": float(d.get("bf16_tflops_sustained", d["bf16_tflops"])),
+                "source": "measured (MEASURED_PEAKS.json)"}
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0,
+                "source": "fallback (earlier measurement on this pool; MEASURED_PEAKS.json absent)"}
 
 
-def sample_text(t_sample: float, scale: float) -> str:
-    return (f"oracle (C++ restatement of the reference, OpenMP) factor + direct solve of the c3 sphere at f=4 GHz "
-            f"on icosphere {CPU_SAMPLE['sub']} (N=1,920, leaf {CPU_SAMPLE['leaf']}, 3 levels, ACA 1e-5, RRQR 1e-7) "
-            f"= {t_sample:.2f} s, scaled to the workload by factorization flops x{scale:.1f}")
+def config_block(cfg, world):
+    """The `config` object of both arms (identical, so the driver can pair them)."""
+    return {"workload": cfg["desc"], "N": cfg.get("N"), "nrhs": cfg["nrhs"],
+            "parallelism": "replicas" if world > 1 else "single GPU",
+            "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"}
 
 
 def run_reference(args, rank, world):
-    """Reference arm: the reference's algorithm on the host CPU (the oracle
-    port; the reference itself needs Eigen 3, absent here), timed on a bounded
-    sample and scaled to the workload by algorithmic factorization flops."""
+    """Reference arm: the reference's CPU algorithm (the oracle) on the host
+    cores, all threads, on bounded samples of the workload's own tree,
+    extrapolated to the workload (a lower bound; see CPUBaseline).  Loads no
+    GPU library.  Rank 0 only."""
     if rank != 0:
         return
     cfg = CONFIGS[args.config]
     threads = os.cpu_count() or 1
-    from rcs_b200.kernel import Context
-    ctx = Context(0)
-    scale = factor_flops(cfg, ctx) / factor_flops(CPU_SAMPLE, ctx)
-    times = []
-    for _ in range(min(args.warmup, 1)):
-        cpu_sample_seconds(threads)
-    for _ in range(args.steps):
-        times.append(cpu_sample_seconds(threads))
-    t_s = float(np.mean(times))
-    v = t_s * scale
+    t_setup = time.perf_counter()
+    cb = CPUBaseline(cfg)
+    t_setup = time.perf_counter() - t_setup
+    for i in range(args.warmup):
+        cb.sample(i, threads)
+    recs = []
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        recs.append(cb.sample(args.warmup + i, threads)[1])
+    t_timed = time.perf_counter() - t0
+    v = cb.extrapolate(recs, cb.lu_macs, cb.pair_macs)
+    # the reference factorizes on one thread (test/sphere.cpp:206-207): one more sample at 1 thread
+    r1 = cb.sample(args.warmup + args.steps, 1)[1]
+    v1 = cb.extrapolate([r1], cb.lu_macs, cb.pair_macs)
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": v * 1e3, "higher_is_better": False, "scaling": "weak",
-            "vs_baseline": None, "dtype": "c128", "data": "synthetic",
-            "config": {"workload": cfg["desc"], "parallelism": "replicas" if world > 1 else "single process",
-                       "reference_path": "factor + direct solve at the config's ACA/RRQR tolerances (the reference "
-                                         "has no refinement)"},
+            "vs_baseline": None, "dtype": "c128", "data": "synthetic", "config": config_block(cfg, world),
+            "extrapolated": "lower bound",
+            "reference_path": "the reference's factorization (the oracle restates it; Eigen 3 is absent) on the host "
+                              "CPU; no refinement",
             "cpu_baseline": {"value": v, "unit": "s", "cores": threads, "kind": "port",
-                             "sample": sample_text(t_s, scale)},
+                             "sample": cb.describe(recs, threads)},
+            "single_thread": {"value": v1, "unit": "s", "cores": 1, "sample": cb.describe([r1], 1)},
+            "samples": recs, "timed_region_s": t_timed, "setup_s": t_setup,
             "e2e": {"value": v, "unit": "s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -286,10 +354,11 @@ def main():
         return
     import torch
     torch.cuda.set_device(local)
-    from rcs_b200.solver import launch_count, profile_gemm, profile_gemm_read
+    from rcs_b200.solver import launch_count, profile_gemm, profile_gemm_table
     cfg = CONFIGS[args.config]
     ctx, m, K, S, A, B, t_asm, t_op = build_workload(cfg, local)
     N, nrhs = K.N, B.shape[1]
+    assert N == cfg["N"], "the mesh does not have the configuration's unknown count"
     stream = torch.cuda.ExternalStream(ctx.stream(), device=local)
     Bd = torch.from_numpy(np.ascontiguousarray(B.T)).to(f"cuda:{local}")  # nrhs x N == column-major N x nrhs
     Xd = torch.empty_like(Bd)
@@ -331,16 +400,18 @@ def main():
               "matvec_s_per_step": float(np.mean([r["t_matvec"] for r in recs]))}
 
     # e2e: the public host API, pinned host buffers, H2D/D2H inside the step
+    # (a few steps: the same work as `value`, through the host-buffer call)
     Bh = torch.from_numpy(np.ascontiguousarray(B.T)).pin_memory()
     Xh = torch.empty_like(Bh).pin_memory()
     from rcs_b200 import _lib
     import ctypes as C
     hb = np.ctypeslib.as_array(C.cast(Bh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))
     hx = np.ctypeslib.as_array(C.cast(Xh.data_ptr(), C.POINTER(C.c_double)), shape=(2 * N * nrhs,))
+    e2e_steps = min(args.steps, 3)
     barrier(world)
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(e2e_steps):
         S.rewind()
         _lib.check(_lib.lib().aifmm_solver_factorize(S.h))
         if A is None:
@@ -349,17 +420,41 @@ def main():
             gi = _lib.GmresInfo()
             _lib.check(_lib.lib().aifmm_solver_solve_gmres(S.h, A.h, hb, nrhs, hx, float(cfg["gmres"]), 30, 300,
                                                            C.byref(gi)))
-    t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps, world)
+    t_e2e = max_over_ranks((time.perf_counter() - t0) / e2e_steps, world)
     res_e2e = sampled_residual(K, Xh.numpy().T, B, nrows=512)
 
-    # roofline of the dominant kernel (grouped complex GEMM) over one more step
+    # device time of every grouped-GEMM launch and RRQR chain of one more
+    # step, by call site (CUDA events on the library stream around each launch)
     profile_gemm(True)
     step()
     torch.cuda.synchronize()
-    g_ms, g_flops, g_n = profile_gemm_read()
+    table = profile_gemm_table()
     profile_gemm(False)
-    peak = zgemm_peak_tflops()
-    achieved = g_flops / (g_ms / 1e3) / 1e12 if g_ms > 0 else 0.0
+    pk = peaks()
+    zpeak = zgemm_peak_tflops()
+    phases = {}
+    for tag, n, sec, fl in table:
+        if not tag.startswith("gemm:"):
+            continue
+        prec = int(tag.split(":")[1])
+        key = "tcgen05 split-TF32 GEMM" if prec >= 2 else "FP64 GEMM"
+        ph = phases.setdefault(key, {"launches": 0, "device_s": 0.0, "flops": 0.0})
+        ph["launches"] += n
+        ph["device_s"] += sec
+        ph["flops"] += fl
+    for key, ph in phases.items():
+        ph["tflops"] = ph["flops"] / ph["device_s"] / 1e12 if ph["device_s"] > 0 else 0.0
+        if key.startswith("tcgen05"):
+            ph["peak_tflops"] = pk["bf16_tflops_sustained"]
+            ph["peak"] = "dense bf16 sustained, " + pk["source"]
+            ph["tf32_issued_tflops"] = 3.0 * ph["tflops"]
+        else:
+            ph["peak_tflops"] = zpeak
+            ph["peak"] = "cuBLAS complex128 GEMM 4096^3 measured on this GPU"
+        ph["frac"] = ph["tflops"] / ph["peak_tflops"] if ph["peak_tflops"] else None
+    rrqr_s = sum(sec for tag, n, sec, fl in table if tag.startswith("rrqr:"))
+    tc = phases.get("tcgen05 split-TF32 GEMM")
+    dom = tc if tc else phases.get("FP64 GEMM", {"tflops": 0.0, "peak_tflops": zpeak, "frac": None, "launches": 0})
 
     # the plain FP64 factorization on the same workload and refinement: one
     # warm-up and one timed step, for the mixed-vs-plain comparison
@@ -399,24 +494,23 @@ def main():
     cpu = None
     if rank == 0 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        t_s = cpu_sample_seconds(threads)
-        scale = info["flops_factor"] / max(factor_flops(CPU_SAMPLE, ctx), 1.0)
-        cpu = {"value": t_s * scale, "unit": "s", "cores": threads, "kind": "port", "sample": sample_text(t_s, scale)}
+        cb = CPUBaseline(cfg)
+        recs_cpu = [cb.sample(i, threads)[1] for i in range(3)]
+        v = cb.extrapolate(recs_cpu, cb.lu_macs, cb.pair_macs)
+        cpu = {"value": v, "unit": "s", "cores": threads, "kind": "port", "extrapolated": "lower bound",
+               "sample": cb.describe(recs_cpu, threads)}
     if rank == 0:
         line = {
             "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "c128" if cfg.get("precision", 0) == 0 else "c128+tf32x3",
             "data": "synthetic",
-            "config": {"workload": cfg["desc"], "N": N, "nrhs": nrhs,
-                       "path": ({0: "plain complex128 factorization (reference control flow)",
-                                 1: "mixed factorization (split-TF32 mma.sync GEMMs)",
-                                 2: "mixed factorization (split-TF32 tcgen05 GEMMs)",
-                                 3: "mixed factorization (split-TF32 tcgen05 GEMMs, pre-tiled planes)"}
-                                [cfg.get("precision", 0)]
-                                + (" + FP64 FGMRES" if A is not None else ", direct solve")),
-                       "parallelism": "replicas" if world > 1 else "single GPU",
-                       "l2": "inputs larger than L2 (leaf blocks and fill-ins stream from HBM)"},
+            "config": config_block(cfg, world),
+            "path": ({0: "plain complex128 factorization (reference control flow)",
+                      1: "mixed factorization (split-TF32 mma.sync GEMMs)",
+                      2: "mixed factorization (split-TF32 tcgen05 GEMMs)",
+                      3: "mixed factorization (split-TF32 tcgen05 GEMMs, pre-tiled planes)"}[cfg.get("precision", 0)]
+                     + (" + FP64 FGMRES" if A is not None else ", direct solve")),
             "residual": res, "residual_e2e": res_e2e, "residual_rows_sampled": min(2048, N),
             "residual_reference": "||Z x - b|| / ||b|| over seeded rows with exact FP64 matrix entries",
             "gmres": gm, "plain_fp64": plain, "assemble_s": t_asm, "operator_build_s": t_op,
@@ -426,15 +520,15 @@ def main():
             "tree": {"levels": info["n_levels"], "avg_leaf": info["avg_leaf_size"], "avg_rank": info["avg_multipoles"],
                      "max_rank": info["max_rank"], "rrqr": info["n_rrqr"]},
             "gpu_launches": int(launches),
-            "roofline": {"bound": "tensor", "kernel": "grouped GEMM launches of the step (FP64 zgemm_grouped_kernel "
-                                                "and, on the mixed path, the tcgen05 Schur products)",
-                         "achieved": achieved,
-                         "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak if peak else None,
-                         "peak_source": "measured cuBLAS complex128 GEMM 4096^3 on this GPU (FP64 path; "
-                                        "MEASURED_PEAKS.json has no FP64 figure)",
-                         "traffic": None, "launches_profiled": g_n},
+            "roofline": {"bound": "tensor",
+                         "kernel": ("zgemm_tc5p_kernel (tcgen05 split-TF32 Schur products; complex-counted "
+                                    "8 m n k flops per product)") if tc else "zgemm_grouped_kernel (FP64)",
+                         "achieved": dom["tflops"], "peak": dom["peak_tflops"], "unit": "TFLOP/s",
+                         "frac": dom["frac"], "peak_source": dom.get("peak", ""),
+                         "traffic": None, "launches_profiled": dom["launches"]},
+            "roofline_phases": {**phases, "RRQR chains": {"device_s": rrqr_s}},
             "clocks": clk.summary(),
-            "e2e": {"value": t_e2e, "unit": "s", "h2d_bytes_per_step": int(16 * N * nrhs),
+            "e2e": {"value": t_e2e, "unit": "s", "steps": e2e_steps, "h2d_bytes_per_step": int(16 * N * nrhs),
                     "d2h_bytes_per_step": int(16 * N * nrhs)},
             "cpu_baseline": cpu,
         }

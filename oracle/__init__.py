@@ -70,6 +70,11 @@ def lib():
             "or_aifmm_leaf_counts": (_i, [_p, _ip]),
             "or_efie_set_plane_projection": (None, [_p, _i]),
             "or_aifmm_dump": (C.c_long, [_p, _p, C.c_long]),
+            "or_tree_shape_create": (_p, [_p, _dp, _i, _i, _dp]),
+            "or_tree_shape_sizes": (None, [_p, _ip]),
+            "or_tree_shape_get": (None, [_p, _ip, _ip, _ip, _ip]),
+            "or_tree_shape_destroy": (None, [_p]),
+            "or_schur_sample": (_i, [_p, _ip, _i, _ip, _ip, _i, _ip, _i, _i, _dp, _dp]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -246,3 +251,45 @@ class AIFMM:
                     maxRank=int(i[4]), nRRQR=int(i[5]), nCompressP2P=int(i[6]), nCompressP2L=int(i[7]),
                     t_assemble=float(t[0]), t_factor=float(t[1]), t_solve=float(t[2]),
                     mem_GB=float(m[0]), mem_after_GB=float(m[1]))
+
+
+def tree_shape(kernel: Kernel, leaf_size: int, n_levels: int = 0):
+    """The reference's tree over the kernel's locations without skeletons:
+    (n_levels, leaf point lists, leaf neighbour lists), leaves in box order."""
+    loc = kernel.locations()
+    bbox = np.array([loc[:, 0].min(), loc[:, 0].max(), loc[:, 1].min(), loc[:, 1].max(),
+                     loc[:, 2].min(), loc[:, 2].max()], dtype=np.float64)
+    h = lib().or_tree_shape_create(kernel.h, bbox, int(leaf_size), int(n_levels), np.ascontiguousarray(loc).ravel())
+    if not h:
+        raise RuntimeError("oracle: " + lib().or_last_error().decode())
+    try:
+        sz = np.zeros(3, dtype=np.int32)
+        lib().or_tree_shape_sizes(h, sz)
+        nl, nleaf, nnb = (int(v) for v in sz)
+        po = np.zeros(nleaf + 1, dtype=np.int32)
+        pts = np.zeros(max(kernel.N, 1), dtype=np.int32)
+        no = np.zeros(nleaf + 1, dtype=np.int32)
+        nbi = np.zeros(max(nnb, 1), dtype=np.int32)
+        lib().or_tree_shape_get(h, po, pts, no, nbi)
+    finally:
+        lib().or_tree_shape_destroy(h)
+    leaves = [pts[po[b]:po[b + 1]].copy() for b in range(nleaf)]
+    nbs = [nbi[no[b]:no[b + 1]].copy() for b in range(nleaf)]
+    return nl, leaves, nbs
+
+
+def schur_sample(kernel: Kernel, box_pts, nb_pts: list, pairs, threads: int):
+    """Times the reference's leaf-level near-field Schur updates of one box
+    (LU of P2P[k][k]; P2P[nn][pp] -= P2P[nn][k] lu.solve(P2P[k][pp]) per pair)
+    on `threads` threads.  Returns (seconds_lu, seconds_pairs, macs_lu,
+    macs_pairs)."""
+    bp = np.ascontiguousarray(box_pts, dtype=np.int32)
+    off = np.zeros(len(nb_pts) + 1, dtype=np.int32)
+    off[1:] = np.cumsum([len(v) for v in nb_pts])
+    flat = np.ascontiguousarray(np.concatenate(nb_pts) if nb_pts else np.zeros(1), dtype=np.int32)
+    pr = np.ascontiguousarray(np.asarray(pairs, dtype=np.int32).ravel())
+    sec = np.zeros(2)
+    macs = np.zeros(2)
+    _check(lib().or_schur_sample(kernel.h, bp, len(bp), off, flat, len(nb_pts), pr, len(pr) // 2, int(threads), sec,
+                                 macs))
+    return float(sec[0]), float(sec[1]), float(macs[0]), float(macs[1])

@@ -299,3 +299,127 @@ extern "C" long or_aifmm_dump(void* sp, double* out, long cap) {
     }
   return n;
 }
+
+// ------------------------------------------------------------ CPU baseline sample
+// The reference's tree geometry without skeletons (T:52-165, :167-331,
+// :425-463, :576-625): leaf boxes with their charges and neighbour lists.
+// Used by the CPU-baseline leg of bench.py to size its extrapolation; no
+// kernel entry is evaluated.
+namespace {
+struct Shape {
+  int nLevels = 0;
+  std::vector<int> ptOff, pts, nbOff, nbIdx;
+};
+}  // namespace
+
+extern "C" void* or_tree_shape_create(void* k, const double* bbox, int leafSize, int nLevelsInput,
+                                      const double* locations) {
+  try {
+    Kernel* K = static_cast<Kernel*>(k);
+    SolverInputs in;
+    in.xmin = bbox[0]; in.xmax = bbox[1];
+    in.ymin = bbox[2]; in.ymax = bbox[3];
+    in.zmin = bbox[4]; in.zmax = bbox[5];
+    in.leafSize = leafSize;
+    in.tol_pow = 5;
+    in.nLevelsInput = nLevelsInput;
+    in.fillin_rank = 0;
+    in.fillin_tol = 7;
+    in.locations.resize(K->N);
+    for (int i = 0; i < K->N; ++i)
+      in.locations[i] = V3(locations[3 * i], locations[3 * i + 1], locations[3 * i + 2]);
+    Tree t(in, K, false);
+    t.createTree();
+    t.assign_Center_Location();
+    t.assign_Tree_Interactions();
+    t.assignChargeLocations();
+    auto* s = new Shape;
+    s->nLevels = t.nLevels;
+    const auto& leaves = t.tree[t.nLevels];
+    s->ptOff.push_back(0);
+    s->nbOff.push_back(0);
+    for (const Box& B : leaves) {
+      s->pts.insert(s->pts.end(), B.chargeLocations.begin(), B.chargeLocations.end());
+      s->ptOff.push_back((int)s->pts.size());
+      s->nbIdx.insert(s->nbIdx.end(), B.neighborList.begin(), B.neighborList.end());
+      s->nbOff.push_back((int)s->nbIdx.size());
+    }
+    return s;
+  } catch (const std::exception& e) {
+    guard(e);
+    return nullptr;
+  }
+}
+// sizes[0..2] = nLevels, leaf boxes, total neighbour entries
+extern "C" void or_tree_shape_sizes(void* h, int* sizes) {
+  Shape* s = static_cast<Shape*>(h);
+  sizes[0] = s->nLevels;
+  sizes[1] = (int)s->ptOff.size() - 1;
+  sizes[2] = (int)s->nbIdx.size();
+}
+extern "C" void or_tree_shape_get(void* h, int* ptOff, int* pts, int* nbOff, int* nbIdx) {
+  Shape* s = static_cast<Shape*>(h);
+  std::memcpy(ptOff, s->ptOff.data(), sizeof(int) * s->ptOff.size());
+  std::memcpy(pts, s->pts.data(), sizeof(int) * s->pts.size());
+  std::memcpy(nbOff, s->nbOff.data(), sizeof(int) * s->nbOff.size());
+  std::memcpy(nbIdx, s->nbIdx.data(), sizeof(int) * s->nbIdx.size());
+}
+extern "C" void or_tree_shape_destroy(void* h) { delete static_cast<Shape*>(h); }
+
+// Times the leaf-level near-field Schur updates of the reference's
+// eliminate_x (T:3800-4042) for one box k on `threads` OpenMP threads: the LU
+// of P2P[k][k] (Eigen::PartialPivLU in the reference) and, for every listed
+// pair of neighbours (nn, pp) that are not yet eliminated,
+//     P2P[nn][pp] = P2P[nn][pp] - P2P[nn][k] * lu.solve(P2P[k][pp])
+// with the solve recomputed for every pair, as the reference does.  The
+// blocks P2P[k][k], P2P[nn][k] and P2P[k][pp] are assembled from the kernel
+// before the clock starts; the targets start at zero (their values do not
+// change the work).  nb lists the neighbours' charges (CSR: nbOff, nbPts);
+// pairs holds npairs (a, b) index pairs into that list.  seconds[0] and
+// macs[0] are the LU's, seconds[1] and macs[1] the pair updates' (complex
+// multiply-adds: m^3 / 3 per LU, m^2 n per solve, m n k per product).
+extern "C" int or_schur_sample(void* k, const int* boxPts, int mk, const int* nbOff, const int* nbPts, int nnb,
+                               const int* pairs, int npairs, int threads, double* seconds, double* macs) {
+  try {
+    Kernel* K = static_cast<Kernel*>(k);
+    std::vector<int> kp(boxPts, boxPts + mk);
+    std::vector<std::vector<int>> nb(nnb);
+    for (int a = 0; a < nnb; ++a) nb[a].assign(nbPts + nbOff[a], nbPts + nbOff[a + 1]);
+    Mat Pkk = K->getMatrix(kp, kp);
+    std::vector<Mat> Pnk(nnb), Pkp(nnb);
+    std::vector<bool> needN(nnb, false), needP(nnb, false);
+    for (int q = 0; q < npairs; ++q) {
+      needN[pairs[2 * q]] = true;
+      needP[pairs[2 * q + 1]] = true;
+    }
+    for (int a = 0; a < nnb; ++a) {
+      if (needN[a]) Pnk[a] = K->getMatrix(nb[a], kp);
+      if (needP[a]) Pkp[a] = K->getMatrix(kp, nb[a]);
+    }
+    std::vector<Mat> T(npairs);
+    for (int q = 0; q < npairs; ++q) T[q] = Mat::Zero((int)nb[pairs[2 * q]].size(), (int)nb[pairs[2 * q + 1]].size());
+    const int saved = omp_get_max_threads();
+    omp_set_num_threads(threads);
+    const double t0 = omp_get_wtime();
+    LU lu(Pkk);
+    const double t1 = omp_get_wtime();
+    for (int q = 0; q < npairs; ++q) {
+      const int a = pairs[2 * q], b = pairs[2 * q + 1];
+      T[q] = T[q] - Pnk[a] * lu.solve(Pkp[b]);
+    }
+    const double t2 = omp_get_wtime();
+    omp_set_num_threads(saved);
+    seconds[0] = t1 - t0;
+    seconds[1] = t2 - t1;
+    macs[0] = (double)mk * mk * mk / 3.0;
+    double m = 0;
+    for (int q = 0; q < npairs; ++q) {
+      const double mn = (double)nb[pairs[2 * q]].size(), mp = (double)nb[pairs[2 * q + 1]].size();
+      m += (double)mk * mk * mp + mn * mk * mp;
+    }
+    macs[1] = m;
+    return 0;
+  } catch (const std::exception& e) {
+    return guard(e);
+  }
+}
