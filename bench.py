@@ -44,6 +44,12 @@ CONFIGS = {
                desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
                     "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs over pre-tiled "
                     "planes) as the preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
+    "c2": dict(N=81920, kind="es", sub=6, radius=1.0, leaf=128, tol_pow=5, fillin_tol=7, nrhs=33, levels=0,
+               op_tol=10, gmres=1e-8, precision=3,
+               desc="Electrostatics unit sphere, 81,920 flat triangles (piecewise-constant charge, collocation at "
+                    "centroids), leaf 128, ACA 1e-5, RRQR 1e-7, 32 seeded N(0,1) potentials + the 1 V conductor "
+                    "RHS, mixed factorization (split-TF32 tcgen05 GEMMs, FP32-class) as the preconditioner of FP64 "
+                    "FGMRES(30) to 1e-8 on an ACA-1e-10 H2 operator; capacitance vs 4 pi eps0 R"),
     "c3s": dict(N=30720, sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
                 gmres=1e-6, precision=3,
                 desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
@@ -66,6 +72,23 @@ def plane_waves(n: int, seed: int = 4):
         e_ph = np.array([-math.sin(ph), math.cos(ph), 0.0])
         out.append((k, (e_th if q % 2 == 0 else e_ph).astype(np.complex128)))
     return out
+
+
+def es_rhs(K, n_random: int, seed: int = 20261203) -> np.ndarray:
+    """Electrostatics right-hand sides: n_random seeded N(0,1) potential
+    vectors (one per column) and the 1 V conductor right-hand side last
+    (ElectrostaticsMatrix::getRhs)."""
+    rng = np.random.Generator(np.random.MT19937(seed))
+    R = rng.standard_normal((K.N, n_random))
+    return np.concatenate([R, K.getRhs(1)[:, None]], axis=1).astype(np.complex128)
+
+
+def capacitance_error(mesh, sigma: np.ndarray, radius: float) -> float:
+    """C / (4 pi eps0 R) - 1 for the 1 V charge density (getCapacitance,
+    src/ElectrostaticsMatrix.cpp:366-402: total charge over the potential)."""
+    v = mesh.nodes[mesh.tris - 1]
+    area = 0.5 * np.linalg.norm(np.cross(v[:, 1] - v[:, 0], v[:, 2] - v[:, 0]), axis=1)
+    return float(np.real(sigma) @ area) / (4 * np.pi * 8.854187817e-12 * radius) - 1.0
 
 
 class ClockSampler:
@@ -141,13 +164,17 @@ def build_workload(cfg, device: int):
     when the config refines, the FP64 forward operator.  Not timed as a step:
     the reference times assembly separately from factor+solve."""
     from rcs_b200 import mesh as M
-    from rcs_b200.kernel import Context, EFIEMatrix
+    from rcs_b200.kernel import Context, EFIEMatrix, ElectrostaticsMatrix
     from rcs_b200.solver import AIFMM, H2Operator
     ctx = Context(device)
     m = M.icosphere(cfg["sub"], cfg["radius"])
-    K = EFIEMatrix(m, cfg["freq"], ctx=ctx)
-    waves = plane_waves(cfg["nrhs"]) if cfg["nrhs"] > 1 else [(np.array([0.0, 0, -1]), np.array([1, 0, 0j]))]
-    B = np.stack([K.planeWaveRhs(k, e) for k, e in waves], axis=1)
+    if cfg.get("kind", "efie") == "es":
+        K = ElectrostaticsMatrix(m, ctx=ctx)
+        B = es_rhs(K, cfg["nrhs"] - 1)
+    else:
+        K = EFIEMatrix(m, cfg["freq"], ctx=ctx)
+        waves = plane_waves(cfg["nrhs"]) if cfg["nrhs"] > 1 else [(np.array([0.0, 0, -1]), np.array([1, 0, 0j]))]
+        B = np.stack([K.planeWaveRhs(k, e) for k, e in waves], axis=1)
     t0 = time.perf_counter()
     S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"],
               precision=cfg.get("precision", 0))
@@ -514,6 +541,8 @@ def main():
             "residual": res, "residual_e2e": res_e2e, "residual_rows_sampled": min(2048, N),
             "residual_reference": "||Z x - b|| / ||b|| over seeded rows with exact FP64 matrix entries",
             "gmres": gm, "plain_fp64": plain, "assemble_s": t_asm, "operator_build_s": t_op,
+            "capacitance_error": (capacitance_error(m, X[:, -1], cfg["radius"])
+                                  if cfg.get("kind", "efie") == "es" else None),
             "operator_gb": (A.info()["bytes"] / 1e9) if A is not None else None,
             "factor_flops": info["flops_factor"],
             "phases_s": {k: info[k] for k in ("t_rrqr", "t_compress", "t_elim_x", "t_elim_z", "t_nonleaf")},

@@ -208,6 +208,10 @@ typedef struct {
   /* inside eliminate_x/z: box LU factorizations, their multi-column solves,
    * the Schur-complement GEMM launches */
   double t_lu, t_msolve, t_schur;
+  /* ACA phase of the build: host seconds, workspace bytes allocated over all
+   * launches (reruns included), number of launches */
+  double t_aca, aca_ws_bytes;
+  long n_aca_launches;
 } aifmm_solver_info;
 
 /* AIFMM<K>::AIFMM(inputsToSolverClass, K*) (src/AIFMM.cpp:7-93): builds the
@@ -283,6 +287,47 @@ int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* r
 /* Same with device pointers (complex128, n x nrhs, ld = n). */
 int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const void* rhs_device, int nrhs,
                                     void* x_device, double tol, int restart, int maxit, aifmm_gmres_info* info);
+
+/* ---- Learned rank prediction (no counterpart in the reference) ----
+ * A 6 -> 64 -> 64 -> 1 perceptron (ReLU) with BF16 weights, FP32 activations
+ * and FP32 accumulation that predicts log2(1 + rank) of a box's ACA skeleton
+ * (LowRank::ACA_only_nodes2, src/ACA.cpp:639-859) from six features: mean
+ * centre distance to the interaction-list boxes over the box side,
+ * wavenumber times the box side, log2(1 + rows), log2(1 + columns), tree
+ * level, leaf flag.  Training and inference run as this library's own CUDA
+ * kernels.  Parameter layout (aifmm_mlp_num_params floats): W1 [64 x 6]
+ * row-major, b1 [64], W2 [64 x 64] row-major (output, input), b2 [64],
+ * w3 [64], b3. */
+typedef struct aifmm_mlp aifmm_mlp;
+int aifmm_mlp_num_params(int* n);
+/* Seeded He initialisation, zero biases, identity normalisation. */
+int aifmm_mlp_create(aifmm_ctx* ctx, unsigned long long seed, aifmm_mlp** out);
+int aifmm_mlp_destroy(aifmm_mlp* m);
+/* Inputs are normalised on the device as (x - mean) * scale (6 floats each). */
+int aifmm_mlp_set_normalization(aifmm_mlp* m, const float* mean, const float* scale);
+int aifmm_mlp_get_params(aifmm_mlp* m, float* params);
+int aifmm_mlp_set_params(aifmm_mlp* m, const float* params);
+/* y[i] = prediction for the raw features X[6 i .. 6 i + 5]. */
+int aifmm_mlp_infer(aifmm_mlp* m, const float* X, int n, float* y);
+/* Gradient of the mean squared error (1/n) sum (y_i - t_i)^2 at the current
+ * parameters (the BF16 rounding of the FP32 master weights), and the loss. */
+int aifmm_mlp_grad(aifmm_mlp* m, const float* X, const float* t, int n, float* grad, float* loss);
+/* Full-batch Adam (lr, beta 0.9 / 0.999) on the mean squared error for
+ * `epochs` steps; loss_first / loss_last: the loss before the first and the
+ * last step (either may be NULL). */
+int aifmm_mlp_train(aifmm_mlp* m, const float* X, const float* t, int n, int epochs, float lr, float* loss_first,
+                    float* loss_last);
+/* Solvers created on ctx afterwards size each box's ACA workspace from the
+ * model's prediction times `margin` (plus 8 terms) instead of the fixed
+ * bound of 128; a box whose ACA needs more terms is rerun with twice the
+ * bound, so the ranks are the plain ACA's either way.  The context keeps a
+ * copy of the model; m = NULL restores the fixed bound. */
+int aifmm_ctx_set_rank_model(aifmm_ctx* ctx, const aifmm_mlp* m, double margin);
+/* The ACA problems of the solver's build, in launch order: raw features
+ * (n x 6 floats), the rank bound each was first launched with, and the
+ * rank the ACA found.  *n receives the count; at most cap records are
+ * written. */
+int aifmm_solver_aca_log(aifmm_solver* s, float* features, int* rmax0, int* ranks, int cap, int* n);
 
 /* Per-operation accounting of the solver's host-driven factorization and
  * solve (diagnosis only): on = 1 clears and starts it -- every accounted

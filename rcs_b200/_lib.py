@@ -23,6 +23,7 @@ _p = C.c_void_p
 _pp = C.POINTER(C.c_void_p)
 _ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 
 # name -> (restype, argtypes); every function returns an int status.
 SIGNATURES = {
@@ -57,6 +58,17 @@ SIGNATURES = {
     "aifmm_launch_count": (_i, [C.POINTER(C.c_long)]),
     "aifmm_tc5_timeouts": (_i, [C.POINTER(C.c_long)]),
     "aifmm_debug_gemm_hold": (_i, [_p, _i]),
+    "aifmm_mlp_num_params": (_i, [C.POINTER(_i)]),
+    "aifmm_mlp_create": (_i, [_p, C.c_ulonglong, _pp]),
+    "aifmm_mlp_destroy": (_i, [_p]),
+    "aifmm_mlp_set_normalization": (_i, [_p, _fp, _fp]),
+    "aifmm_mlp_get_params": (_i, [_p, _fp]),
+    "aifmm_mlp_set_params": (_i, [_p, _fp]),
+    "aifmm_mlp_infer": (_i, [_p, _fp, _i, _fp]),
+    "aifmm_mlp_grad": (_i, [_p, _fp, _fp, _i, _fp, C.POINTER(C.c_float)]),
+    "aifmm_mlp_train": (_i, [_p, _fp, _fp, _i, _i, C.c_float, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+    "aifmm_ctx_set_rank_model": (_i, [_p, _p, _d]),
+    "aifmm_solver_aca_log": (_i, [_p, _p, _p, _p, _i, C.POINTER(_i)]),
     "aifmm_profile_ops": (_i, [_i]),
     "aifmm_profile_ops_read": (_i, [C.c_char_p, _i]),
     "aifmm_aca": (_i, [_p, _ip, _i, _ip, _i, _d, _ip, _ip, C.POINTER(_i), _dp, _dp]),
@@ -94,7 +106,8 @@ class SolverInfo(C.Structure):
                 ("mem_gb", C.c_double), ("mem_after_gb", C.c_double), ("t_rrqr", C.c_double),
                 ("t_compress", C.c_double), ("t_elim_x", C.c_double), ("t_elim_z", C.c_double),
                 ("t_nonleaf", C.c_double), ("t_lu", C.c_double), ("t_msolve", C.c_double),
-                ("t_schur", C.c_double)]
+                ("t_schur", C.c_double), ("t_aca", C.c_double), ("aca_ws_bytes", C.c_double),
+                ("n_aca_launches", C.c_long)]
 
 class GmresInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("cycles", C.c_int), ("relres", C.c_double), ("t_precond", C.c_double),

@@ -40,6 +40,10 @@ struct aifmm_ctx {
   // AIFMM_ETIMEOUT.
   bool gemmHold = false;
   int* holdFlag = nullptr;
+  // Rank model used by solvers built on this context to size each box's ACA
+  // workspace (aifmm_ctx_set_rank_model keeps a copy; null: fixed bound).
+  std::shared_ptr<struct aifmm_mlp> rankModel;
+  double rankMargin = 1.25;
   // Sub-allocator for the blocks of 256 KB and more (arena.cuh); its chunks
   // come from `pool`.  Created with the context.
   std::mutex arenaMu;

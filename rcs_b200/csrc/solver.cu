@@ -202,12 +202,32 @@ void Solver::gatherBlocks(const std::vector<std::vector<int>*>& rows, const std:
 }
 
 // ------------------------------------------------------------ skeletons, T:917-1256
+RankFeatures Solver::rankFeatures(int j, int k, int nr, int nc) const {
+  const DBox& B = tree[j][k];
+  double d = 0.0;
+  for (int kIL : B.IL) {
+    const double* a = B.center;
+    const double* b = tree[j][kIL].center;
+    d += std::sqrt((a[0] - b[0]) * (a[0] - b[0]) + (a[1] - b[1]) * (a[1] - b[1]) + (a[2] - b[2]) * (a[2] - b[2]));
+  }
+  RankFeatures f;
+  f.f[0] = B.IL.empty() ? 0.0f : (float)(d / B.IL.size() / boxSideLength[j]);
+  f.f[1] = K->geom.efie ? (float)(K->geom.ge.kappa * boxSideLength[j]) : 0.0f;
+  f.f[2] = (float)std::log2(1.0 + nr);
+  f.f[3] = (float)std::log2(1.0 + nc);
+  f.f[4] = (float)j;
+  f.f[5] = (j == nLevels) ? 1.0f : 0.0f;
+  return f;
+}
+
 void Solver::runACA(int j, bool incoming) {
   struct Item {
     int k;
     std::vector<int> boxA, ILn;
-    int nr, nc, rmax;
+    int nr, nc, rmax, rmax0;
+    RankFeatures feat;
   };
+  const double tAca0 = wall();
   std::vector<Item> items;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
     DBox& B = tree[j][k];
@@ -246,6 +266,27 @@ void Solver::runACA(int j, bool incoming) {
       B.out_charge = it.boxA;
     }
   }
+  // The workspace of a problem holds rmax rank-1 terms.  With a rank model on
+  // the context, its prediction (with a margin) sizes rmax instead of the
+  // fixed bound; either way a problem whose adaptive ACA needs more terms is
+  // rerun with twice the bound (the plain ACA decides the rank).
+  {
+    std::vector<RankFeatures> feats(items.size());
+    for (size_t q = 0; q < items.size(); ++q) feats[q] = rankFeatures(j, items[q].k, items[q].nr, items[q].nc);
+    if (ctx->rankModel && !items.empty()) {
+      std::vector<float> y;
+      mlp_infer(ctx->rankModel.get(), feats, y);
+      for (size_t q = 0; q < items.size(); ++q) {
+        const double pred = std::max(0.0, std::exp2((double)y[q]) - 1.0);
+        const int r = std::max(16, (int)std::ceil(pred * ctx->rankMargin) + 8);
+        items[q].rmax = std::min({r, std::min(items[q].nr, items[q].nc), 1024});
+      }
+    }
+    for (size_t q = 0; q < items.size(); ++q) {
+      items[q].feat = feats[q];
+      items[q].rmax0 = items[q].rmax;
+    }
+  }
   const double tol = std::pow(10, -prm.tol_pow);
   std::vector<Item*> pending;
   for (auto& it : items) pending.push_back(&it);
@@ -281,6 +322,7 @@ void Solver::runACA(int j, bool incoming) {
       const size_t zU = (size_t)it->rmax * nP, zV = (size_t)it->rmax * nS;
       const size_t zAc = (size_t)it->nr * it->rmax, zAr = (size_t)it->rmax * it->nc;
       ws.emplace_back(ctx, sizeof(zd) * (zU + zV + zAc + zAr) + (it->nr + it->nc) + sizeof(int) * 2 * it->rmax + 64);
+      stats.aca_ws_bytes += (double)ws.back().bytes;
       char* base = (char*)ws.back().p;
       ACAProblem P;
       P.rows = dids.as<int>() + offs[q];
@@ -302,6 +344,7 @@ void Solver::runACA(int j, bool incoming) {
     launch_aca(ctx, K->geom, probs, tol);
     stats.kernels++;
     stats.nACA += nq;
+    stats.nACALaunches++;
     std::vector<int> rs(2 * nq);
     AIFMM_CUDA(cudaMemcpyAsync(rs.data(), dint.p, sizeof(int) * 2 * nq, cudaMemcpyDeviceToHost, ctx->stream));
     ops.sync();
@@ -316,6 +359,7 @@ void Solver::runACA(int j, bool incoming) {
         pending.push_back(it);
         continue;
       }
+      acaLog.push_back({it->feat, it->rmax0, rank});
       DBox& B = tree[j][it->k];
       std::vector<int> rb(rank), cb(rank);
       if (rank > 0) {
@@ -345,6 +389,7 @@ void Solver::runACA(int j, bool incoming) {
       }
     }
   }
+  stats.t_aca += wall() - tAca0;
 }
 
 static void truncateTo(std::vector<int>& v, size_t n) {

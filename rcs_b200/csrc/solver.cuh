@@ -12,6 +12,7 @@
 
 #include "dmat.cuh"
 #include "lowrank.cuh"
+#include "mlp.cuh"
 
 namespace aifmm {
 
@@ -31,6 +32,16 @@ struct SolverStats {
   double flops_factor = 0;  // complex-counted algorithmic flops issued by the factorization
   long nRRQR = 0, nRRQRShort = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
   long kernels = 0;
+  double t_aca = 0;          // host time of the ACA phase (launches, retries, read-backs)
+  double aca_ws_bytes = 0;   // ACA workspace bytes allocated over all launches (retries included)
+  long nACALaunches = 0;     // ACA launches (chunks of problems that fit the workspace budget)
+};
+
+// One ACA problem of the build: its features, the workspace rank bound it was
+// first launched with, and the rank the adaptive ACA found.
+struct ACARecord {
+  RankFeatures x;
+  int rmax0, rank;
 };
 
 struct DBox {
@@ -73,6 +84,7 @@ class Solver {
   int fillin_rankVec[64];
   double domain[6];
   bool factored = false;
+  std::vector<ACARecord> acaLog;  // every ACA problem of the build, in launch order
 
   // xyz (N x 3) and dom (xmin, xmax, ymin, ymax, zmin, zmax) replace the
   // kernel's unknown locations and their bounding box when given, as
@@ -99,6 +111,7 @@ class Solver {
   void assignCharges();
   void getNodesLevel(int j);
   void runACA(int j, bool incoming);
+  RankFeatures rankFeatures(int j, int k, int nr, int nc) const;
   void getL2PP2MBox(int j, int k);
   void assembleM2L();
   void initP2PLeaf();

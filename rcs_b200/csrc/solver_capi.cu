@@ -139,6 +139,9 @@ int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
   info->t_lu = S.stats.t_lu;
   info->t_msolve = S.stats.t_msolve;
   info->t_schur = S.stats.t_schur;
+  info->t_aca = S.stats.t_aca;
+  info->aca_ws_bytes = S.stats.aca_ws_bytes;
+  info->n_aca_launches = S.stats.nACALaunches;
   API_END
 }
 
@@ -193,3 +196,36 @@ int aifmm_solver_destroy(aifmm_solver* s) {
 }
 
 }  // extern "C"
+
+int aifmm_solver_aca_log(aifmm_solver* s, float* features, int* rmax0, int* ranks, int cap, int* n) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && n && cap >= 0, AIFMM_EINVAL, "bad argument");
+  const auto& L = s->s->acaLog;
+  *n = (int)L.size();
+  const int w = std::min(cap, (int)L.size());
+  for (int i = 0; i < w; ++i) {
+    if (features) std::memcpy(features + (size_t)MLP_IN * i, L[i].x.f, sizeof(float) * MLP_IN);
+    if (rmax0) rmax0[i] = L[i].rmax0;
+    if (ranks) ranks[i] = L[i].rank;
+  }
+  API_END
+}
+
+int aifmm_ctx_set_rank_model(aifmm_ctx* ctx, const aifmm_mlp* m, double margin) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx, AIFMM_EINVAL, "ctx is NULL");
+  if (!m) {
+    ctx->rankModel.reset();
+    return AIFMM_OK;
+  }
+  AIFMM_REQUIRE(margin >= 1.0 && margin <= 16.0, AIFMM_EINVAL, "margin must lie in [1, 16]");
+  // a value copy bound to this context (not reference-counted: the context owns it)
+  auto c = std::make_shared<aifmm_mlp>();
+  c->ctx = ctx;
+  c->params = m->params;
+  std::memcpy(c->mean, m->mean, sizeof(c->mean));
+  std::memcpy(c->scale, m->scale, sizeof(c->scale));
+  ctx->rankModel = c;
+  ctx->rankMargin = margin;
+  API_END
+}

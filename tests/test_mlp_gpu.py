@@ -1,0 +1,95 @@
+"""The rank model's CUDA kernels against the CPU restatement
+(oracle/mlp.py): gradients, inference, deterministic training; and the
+ablation: solvers that size each box's ACA workspace from the trained model
+find the same ranks as the fixed-bound solver (the adaptive ACA decides
+them) with fewer reruns and less workspace."""
+import numpy as np
+import pytest
+
+from oracle import mlp as om
+from rcs_b200 import mesh as M
+from rcs_b200 import rankmlp
+from rcs_b200.kernel import Context, EFIEMatrix
+from rcs_b200.solver import AIFMM
+
+pytestmark = pytest.mark.gpu
+
+
+def _data(n, seed):
+    rng = np.random.default_rng(seed)
+    X = rng.standard_normal((n, 6)).astype(np.float32) * np.array([2, 3, 1, 1, 1, 0.5], np.float32) + 4
+    t = (0.5 * X[:, 0] - 0.2 * X[:, 1] + np.sin(X[:, 2]) + 0.1 * X[:, 3] * X[:, 4]).astype(np.float32)
+    return X, t
+
+
+def test_gradient_matches_cpu_oracle():
+    m = rankmlp.RankMLP(seed=11)
+    rng = np.random.default_rng(1)
+    m.set_normalization(rng.standard_normal(6) * 0.5 + 4, 0.5 + rng.random(6))
+    X, t = _data(300, 2)
+    g, loss = m.grad(X, t)
+    lo, go = om.library_grad(m.params, X, t, m.mean, m.scale)
+    assert abs(loss - lo) <= 1e-5 * abs(lo)
+    assert np.max(np.abs(g - go)) <= 1e-4 * np.max(np.abs(go)), np.max(np.abs(g - go)) / np.max(np.abs(go))
+    # per parameter block, so that no layer hides behind a larger one
+    for a, b in ((om.W1, om.B1), (om.B1, om.W2), (om.W2, om.B2), (om.B2, om.W3), (om.W3, om.B3)):
+        assert np.max(np.abs(g[a:b] - go[a:b])) <= 1e-4 * max(np.max(np.abs(go[a:b])), 1e-6)
+
+
+def test_inference_matches_cpu_oracle():
+    m = rankmlp.RankMLP(seed=5)
+    X, _ = _data(1000, 3)
+    m.set_normalization(X.mean(0), 1.0 / X.std(0))
+    y = m.infer(X)
+    yo, _ = om.forward(om.bf16_round(m.params).astype(np.float64), X, m.mean, m.scale)
+    assert np.max(np.abs(y - yo)) <= 1e-5 * np.max(np.abs(yo))
+
+
+def test_training_lowers_loss_and_is_deterministic():
+    X, t = _data(700, 4)
+    runs = []
+    for _ in range(2):
+        m = rankmlp.RankMLP(seed=9)
+        l0, l1 = m.fit(X, np.exp2(t - t.min()) - 1, epochs=1201, lr=3e-3)
+        runs.append((l0, l1, m.params))
+    assert runs[0][1] < 0.05 * runs[0][0], runs[0][:2]
+    assert runs[0][0] == runs[1][0] and runs[0][1] == runs[1][1]
+    assert np.array_equal(runs[0][2], runs[1][2])  # bit-identical weights
+
+
+def _build(ctx, sub, freq, leaf):
+    K = EFIEMatrix(M.icosphere(sub, 0.15), freq, ctx=ctx)
+    S = AIFMM(K, leaf_size=leaf, tol_pow=5, fillin_tol=7)
+    X, r0, r = rankmlp.aca_log(S)
+    info = S.info()
+    S.close()
+    K.close()
+    return X, r0, r, info
+
+
+def test_rank_model_ablation():
+    """Trained on the ACA logs of two spheres, applied to a third (a finer
+    mesh at a higher frequency): identical ranks, fewer reruns of boxes whose
+    rank outgrew the workspace bound, less workspace."""
+    ctx = Context(0)
+    Xa, _, ra, _ = _build(ctx, 4, 4.0e9, 32)
+    Xb, _, rb, _ = _build(ctx, 5, 2.0e9, 128)
+    m = rankmlp.RankMLP(ctx, seed=3)
+    l0, l1 = m.fit(np.concatenate([Xa, Xb]), np.concatenate([ra, rb]), epochs=3000, lr=3e-3)
+    assert l1 < 0.1 * l0
+    X0, b0, r0, i0 = _build(ctx, 5, 4.0e9, 128)  # fixed bound
+    rankmlp.set_rank_model(ctx, m, 1.25)
+    try:
+        X1, b1, r1, i1 = _build(ctx, 5, 4.0e9, 128)  # workspace from the model
+    finally:
+        rankmlp.set_rank_model(ctx, None)
+    assert np.array_equal(r0, r1) and np.array_equal(X0, X1)
+    pred = m.predict_rank(X1)
+    rel = np.abs(pred - r1) / np.maximum(r1, 1)
+    print("ranks", r1.min(), np.median(r1), r1.max(), "median rel. error", np.median(rel),
+          "reruns", i0["n_aca_retry"], "->", i1["n_aca_retry"], "workspace GB", i0["aca_ws_bytes"] / 1e9, "->",
+          i1["aca_ws_bytes"] / 1e9, "ACA s", i0["t_aca"], "->", i1["t_aca"])
+    assert np.median(rel) < 0.25
+    assert i1["n_aca_retry"] <= i0["n_aca_retry"]
+    assert i1["aca_ws_bytes"] < i0["aca_ws_bytes"]
+    ctx.close()
