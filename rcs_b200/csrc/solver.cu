@@ -1238,6 +1238,8 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   const long tc0 = prm.precision >= 2 ? tc_timeouts() : 0;
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   stats.flops_factor = 0;
+  baseLU_ = DLU();
+  baseReady_ = false;
   stats.t_rrqr = stats.t_compress = stats.t_elim_x = stats.t_elim_z = stats.t_nonleaf = 0;
   stats.t_lu = stats.t_msolve = stats.t_schur = 0;
   for (int j = nLevels; j >= startLevel; --j) {
@@ -1275,6 +1277,7 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
       eliminateZ(j, k);
     }
   }
+  factorBase(startLevel);
   ops.sync();
   // a tensor-core tile that gave up on a bounded wait left its Schur block unwritten
   if (prm.precision >= 2) tc_check(tc0, "factorize");
@@ -1351,15 +1354,22 @@ void Solver::rhsEliminateZ(int j, int k) {  // T:4115-4148, :4313-4397
   }
 }
 
-void Solver::baseSolve(int j) {  // solve_particles_at_base_level, T:4772-4810
+// The base-level system of solve_particles_at_base_level (T:4772-4810): the
+// M2L blocks of the start level, fixed once the factorization is done.  The
+// reference assembles and factorizes it in every solve; here it is factorized
+// once, at the end of factorize(), and each solve only applies the factors.
+void Solver::factorBase(int j) {
+  opprof::Scope prof_fn_("base_lu", ctx->stream);
   int NM = 0, NL = 0;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
     NM += tree[j][k].NumMultipoles;
     NL += tree[j][k].NumLocals;
   }
+  baseLU_ = DLU();
+  baseReady_ = true;
   if (NL == 0 || NM == 0) return;
   AIFMM_REQUIRE(NL == NM, AIFMM_EINVAL, "base-level system is not square");
-  DMat A = ops.zeros(NL, NM), b = ops.zeros(NL, nrhs_);
+  DMat A = ops.zeros(NL, NM);
   std::vector<CopyProblem> cps;
   int ri = 0;
   for (int r = 0; r < nBoxesPerLevel[j]; ++r) {
@@ -1371,13 +1381,33 @@ void Solver::baseSolve(int j) {  // solve_particles_at_base_level, T:4772-4810
       if (m.size()) cps.push_back({m.p, A.p + (size_t)si * A.ld() + ri, m.r, m.c, m.ld(), A.ld(), 0, ONE});
       si += tree[j][s].NumMultipoles;
     }
+    ri += tree[j][r].NumLocals;
+  }
+  zcopy_grouped(ctx, cps);
+  baseLU_ = ops.factor(A);
+  stats.flops_factor += 8.0 / 3.0 * NL * (double)NL * NL;
+}
+
+void Solver::baseSolve(int j) {  // solve_particles_at_base_level, T:4772-4810
+  int NM = 0, NL = 0;
+  for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
+    NM += tree[j][k].NumMultipoles;
+    NL += tree[j][k].NumLocals;
+  }
+  if (NL == 0 || NM == 0) return;
+  AIFMM_REQUIRE(NL == NM, AIFMM_EINVAL, "base-level system is not square");
+  if (!baseReady_) factorBase(j);
+  AIFMM_REQUIRE(baseLU_.n == NL, AIFMM_EINVAL, "base-level factors do not match the system");
+  DMat b = ops.zeros(NL, nrhs_);
+  std::vector<CopyProblem> cps;
+  int ri = 0;
+  for (int r = 0; r < nBoxesPerLevel[j]; ++r) {
     const DMat& mr = tree[j][r].multipole_rhs;
     if (mr.size()) cps.push_back({mr.p, b.p + ri, mr.r, mr.c, mr.ld(), b.ld(), 0, ONE});
     ri += tree[j][r].NumLocals;
   }
   zcopy_grouped(ctx, cps);
-  DLU f = ops.factor(A);
-  DMat mp = ops.solve(f, b);
+  DMat mp = ops.solve(baseLU_, b);
   int idx = 0;
   for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
     tree[j][k].multipoles = ops.block(mp, idx, 0, tree[j][k].NumMultipoles, nrhs_);
@@ -1507,6 +1537,8 @@ void Solver::rewind() {
   tree = deepCopy(saved_);
   P2Pq.clear();
   P2L_M2P.clear();
+  baseLU_ = DLU();
+  baseReady_ = false;
   factored = false;
 }
 

@@ -142,6 +142,7 @@ class Solver {
   void rhsEliminateX(int j, int k);
   void rhsEliminateZ(int j, int k);
   void baseSolve(int j);
+  void factorBase(int j);
   void backSubstitute();
   void gatherBlocks(const std::vector<std::vector<int>*>& rows, const std::vector<std::vector<int>*>& cols,
                     std::vector<DMat*>& outs);
@@ -153,6 +154,8 @@ class Solver {
   std::vector<int> leafOff_;          // leaf box -> first tree-order position
   std::vector<std::vector<DBox>> saved_;
   bool hasSaved_ = false;
+  DLU baseLU_;             // factors of the base-level system (factorBase)
+  bool baseReady_ = false;
 };
 
 }  // namespace aifmm
