@@ -6,12 +6,16 @@ the H^2 tree, its elimination and solve sweeps), loaded through ctypes.  Only
 ``bench.py`` may import this package, and only as the checker; the product
 library never links it.
 
-Parity status: the reference itself cannot be built here (it needs Eigen 3,
-which is not installed), so no reference outputs exist to pin against.  The
-oracle is pinned against known answers instead: dense LU on the same
+Parity status: pinned against outputs of the reference itself.  The
+reference's unmodified sources build here against the project-written Eigen
+subset (oracle/ref.mk, oracle/ref_driver.cpp); tests/golden/make_ref_golden.py
+records their outputs as tests/golden/ref_*.npz and tests/test_oracle_ref_pin.py
+checks this oracle against them: bit-identical where the factorization makes
+no fill-in recompression, identical ranks of every box and the solution within
+the RRQR tolerance (two levels) or the ACA tolerance (three levels) where it
+does.  The oracle is also pinned against known answers: dense LU on the same
 operator, the analytic sphere capacitance, the Mie series of a PEC sphere,
-RRQR/ACA residuals and the H^2 approximation error ("parity unpinned" against
-reference outputs).
+RRQR/ACA residuals and the H^2 approximation error.
 """
 from __future__ import annotations
 
@@ -38,6 +42,19 @@ def build(force: bool = False) -> str:
     if force or not os.path.exists(_LIB_PATH):
         subprocess.run(["make", "-s", "-C", _HERE], check=True)
     return _LIB_PATH
+
+
+def build_ref(root: str | None = None) -> str | None:
+    """Compile the reference itself into oracle/_ref/aifmm_ref (oracle/ref.mk)
+    when its source tree is present: AIFMM_REFERENCE_ROOT, else the build
+    container's mount at /root/reference.  Returns the binary, or None when the
+    tree is absent (the GPU box has only what was built beforehand)."""
+    root = root or os.environ.get("AIFMM_REFERENCE_ROOT") or "/root/reference"
+    if not os.path.isdir(os.path.join(root, "src")):
+        return None
+    subprocess.run(["make", "-s", "-f", os.path.join(_HERE, "ref.mk"), f"REF={root}", "-j8"], check=True,
+                   cwd=os.path.dirname(_HERE))
+    return os.path.join(_HERE, "_ref", "aifmm_ref")
 
 
 def lib():

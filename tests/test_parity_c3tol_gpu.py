@@ -6,8 +6,16 @@ three levels.  The oracle's outputs come from tests/golden/make_c3tol.py
 (the oracle needs minutes at this size).
 
 Bars: the plain FP64 path reproduces the reference algorithm -- identical
-tree statistics, ranks and recompression counts, solution within 1e-10 of
-the oracle's AIFMM solution -- with either RRQR mode; the mixed path
+tree statistics, ranks and recompression counts with either RRQR mode, and
+the solution within 1e-10 of the oracle's AIFMM solution on the two-level
+tree.  On the three-level tree the non-leaf elimination amplifies rounding:
+the reference itself, built from its own sources, and the oracle agree
+bit for bit on every leaf-level block after factorization and to 1e-15 on the
+level-2 bases, yet their solutions differ by 1.1e-6 (three levels, 1,920
+unknowns, the same tolerances; tests/golden/ref_s1280_l3_t5_f7.npz), because
+the level-2 LU factors and inverses magnify the last-bit differences of the
+basis updates.  The bar there is therefore the integer decisions (ranks,
+counts) plus the ACA tolerance, 1e-5, on the solution.  The mixed path
 (split-TF32 tensor-core Schur products) refined by FP64 FGMRES reaches the
 dense FP64 solution to 1e-6 relative."""
 import os
@@ -22,7 +30,7 @@ from rcs_b200.solver import AIFMM, H2Operator
 pytestmark = pytest.mark.gpu
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "sphere7680_c3tol.npz")
-PARITY = 1e-10
+PARITY = {"leaf128": 1e-10, "lvl3": 1e-5}
 
 
 @pytest.fixture(scope="module")
@@ -51,7 +59,7 @@ def test_plain_matches_oracle(fx, shape, exact):
     assert i["n_rrqr"] == g[f"{shape}_nRRQR"]
     assert i["n_compress_p2p"] == g[f"{shape}_nCompressP2P"] and i["n_compress_p2l"] == g[f"{shape}_nCompressP2L"]
     for c in range(X.shape[1]):
-        assert rel(X[:, c], g[f"{shape}_x"][:, c]) < PARITY
+        assert rel(X[:, c], g[f"{shape}_x"][:, c]) < PARITY[shape]
     S.close()
 
 
