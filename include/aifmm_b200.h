@@ -157,7 +157,9 @@ int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int to
  * precision 0 = FP64 FMA; 1 and 2 = split-TF32 tensor cores with FP32
  * accumulation (FP32 accuracy): 1 by warp-level mma.sync, 2 by tcgen05 with
  * tensor-memory accumulators, 3 by tcgen05 over operands split once into
- * pre-tiled planes streamed with bulk copies.  The dense products of the reference go through Eigen;
+ * pre-tiled planes streamed with bulk copies, 4 by the persistent,
+ * warp-specialised tcgen05 kernel over the real form of the complex product
+ * (128 x 128 complex tiles).  The dense products of the reference go through Eigen;
  * this is the kernel that replaces them on the GPU. */
 int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
@@ -183,14 +185,23 @@ typedef struct {
                     * pivots, norms and solves stay FP64 -- a preconditioner for
                     * aifmm_solver_solve_gmres; 2 = the same with the tcgen05
                     * kernel (tensor-memory accumulators) instead of mma.sync;
-                    * 3 = tcgen05 over operands split once into pre-tiled planes
-                    * (the fastest form) */
+                    * 3 = tcgen05 over operands split once into pre-tiled planes;
+                    * 4 = the persistent, warp-specialised tcgen05 GEMM over
+                    * pre-tiled planes of the real form [Ar Ai][[Br Bi][-Bi Br]]
+                    * (128 x 128 complex tiles, double-buffered accumulators;
+                    * the fastest form) */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
                     * Householder pass, as the reference does; 0 (default) skips
                     * that pass when the old basis is one this solver produced with
                     * orthonormal columns: its partition 1 then keeps every column,
                     * so only the fill-in's component outside the old span is
                     * factorized (same ranks and spans, different rounding) */
+  int drop_pow;    /* fill-in queue threshold of the factorization used as a
+                    * preconditioner: a well-separated fill-in whose norm relative
+                    * to its M2L block is at most 10^-drop_pow is dropped instead
+                    * of recompressed into the bases.  0 (default) = the
+                    * reference's threshold 10^-tol_pow (T:4413, T:4450); a
+                    * negative value drops every such fill-in. */
 } aifmm_solver_params;
 
 typedef struct {
@@ -252,6 +263,15 @@ int aifmm_solver_rewind(aifmm_solver* s);
  * 0 L2P, 1 P2M, 2 M2L, 3 P2P, 4 M2P, 5 P2L, 6 L2P_f, 7 P2M_f, 8 M2M_f, 9 L2M_f.
  * Writes at most cap records; *count receives the total. */
 int aifmm_solver_dump(aifmm_solver* s, double* out, long cap, long* count);
+/* Factorization checkpoint file (no counterpart call in the reference, whose
+ * factors live only in memory: FMM2DTree's per-box blocks,
+ * include/AIFMMBox.hpp:13-71).  save writes a factorized solver -- tree,
+ * index lists, every block and the base-level LU -- to path; load reads one
+ * into a new solver on kernel k (same unknown count), ready for
+ * aifmm_solver_solve* without assembly or factorization.  A loaded solver
+ * cannot refactorize (the assembled operator is not in the file). */
+int aifmm_solver_save(aifmm_solver* s, const char* path);
+int aifmm_solver_load(aifmm_kernel* k, const char* path, aifmm_solver** out);
 
 /* ---- forward operator and FP64 refinement ----------------------------------- */
 /* No counterpart in the reference, which factorizes its tree directly and

@@ -55,6 +55,8 @@ SIGNATURES = {
     "aifmm_solver_destroy": (_i, [_p]),
     "aifmm_solver_checkpoint": (_i, [_p]),
     "aifmm_solver_rewind": (_i, [_p]),
+    "aifmm_solver_save": (_i, [_p, C.c_char_p]),
+    "aifmm_solver_load": (_i, [_p, C.c_char_p, _pp]),
     "aifmm_launch_count": (_i, [C.POINTER(C.c_long)]),
     "aifmm_tc5_timeouts": (_i, [C.POINTER(C.c_long)]),
     "aifmm_debug_gemm_hold": (_i, [_p, _i]),
@@ -94,7 +96,8 @@ SIGNATURES = {
 
 class SolverParams(C.Structure):
     _fields_ = [("leaf_size", C.c_int), ("tol_pow", C.c_int), ("fillin_tol", C.c_int), ("fillin_rank", C.c_int),
-                ("n_levels", C.c_int), ("precision", C.c_int), ("exact_rrqr", C.c_int)]
+                ("n_levels", C.c_int), ("precision", C.c_int), ("exact_rrqr", C.c_int),
+                ("drop_pow", C.c_int)]
 
 
 class SolverInfo(C.Structure):

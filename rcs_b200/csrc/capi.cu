@@ -213,6 +213,7 @@ int aifmm_ctx_create(int device, aifmm_ctx** out) {
   AIFMM_CUDA(cudaSetDevice(device));
   std::unique_ptr<aifmm_ctx> c(new aifmm_ctx);
   c->device = device;
+  AIFMM_CUDA(cudaDeviceGetAttribute(&c->numSMs, cudaDevAttrMultiProcessorCount, device));
   AIFMM_CUDA(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
   cudaMemPoolProps props{};
   props.allocType = cudaMemAllocationTypePinned;

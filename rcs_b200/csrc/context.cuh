@@ -15,6 +15,7 @@
 // not matter to callers.
 struct aifmm_ctx {
   int device = 0;
+  int numSMs = 0;        // streaming multiprocessors of the device (persistent-kernel grids)
   cudaStream_t stream = nullptr;
   cudaMemPool_t pool = nullptr;
   size_t bytes_live = 0;

@@ -522,6 +522,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
   double flops = 0;
   const int mode = ctx->gemmPrecision;
   const int bm = (mode >= 2) ? 128 : GBM;  // row tile of the tcgen05 kernels
+  const int bn = (mode == 4) ? 128 : GBN;  // complex columns per tile
   for (size_t i = 0; i < probs.size();) {
     const int len = chain[i];
     AIFMM_REQUIRE(len >= 1 && i + len <= probs.size(), AIFMM_EINVAL, "bad chain length");
@@ -536,7 +537,7 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
       GemmGroup g;
       g.head = (int)ps.size();
       g.nchain = len;
-      g.tilesN = (h.n + GBN - 1) / GBN;
+      g.tilesN = (h.n + bn - 1) / bn;
       g.tileStart = (int)tiles;
       for (int q = 0; q < len; ++q) {
         ps.push_back(probs[i + q]);
@@ -576,7 +577,9 @@ void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const 
     AIFMM_CUDA(cudaEventCreate(&e1));
     AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
   }
-  if (mode == 3) {
+  if (mode == 4) {
+    zgemm_tc6(ctx, ps, gs);
+  } else if (mode == 3) {
     zgemm_tc5p(ctx, ps, gs, tiles);
   } else if (mode == 2) {
     zgemm_tc5_launch(ctx, a, inl, tiles);

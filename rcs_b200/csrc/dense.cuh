@@ -65,6 +65,12 @@ void tc_wait_args(aifmm_ctx* ctx, GemmArgs& a);
 // Same tiling as zgemm_tc5_launch.
 long zgemm_tc5p_timeouts();
 void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<GemmGroup>& gs, long tiles);
+// The persistent, warp-specialised tensor-core GEMM (zgemm_tc6.cu): complex
+// products as one real product of twice the depth, 128 x 128 complex tiles,
+// double-buffered tensor-memory accumulators.  Groups must be tiled with
+// tilesN = ceil(n / 128) and ceil(m / 128) row tiles.
+long zgemm_tc6_timeouts();
+void zgemm_tc6(aifmm_ctx* ctx, const std::vector<GemmProblem>& ps, const std::vector<GemmGroup>& gs);
 
 // C = alpha op(A) op(B) + beta C for every problem, one launch; the
 // problems must write disjoint C.

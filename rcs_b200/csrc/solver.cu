@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <limits>
 
 #include "h2op.cuh"
 #include "solver.cuh"
@@ -62,6 +63,8 @@ Solver::Solver(aifmm_kernel* k, const SolverParams& p, const double* xyz, const 
     domain[2 * q + 1] = mx[q];
   }
   fillInTolerance = std::pow(10, -1.0 * prm.tol_pow);
+  if (prm.drop_pow > 0) fillInTolerance = std::pow(10, -1.0 * prm.drop_pow);
+  if (prm.drop_pow < 0) fillInTolerance = std::numeric_limits<double>::infinity();
   L = std::max({mx[0] - mn[0], mx[1] - mn[1], mx[2] - mn[2]});
   AIFMM_REQUIRE(prm.leafSize > 0, AIFMM_EINVAL, "leaf size must be positive");
   const int q = N / prm.leafSize;
@@ -1159,6 +1162,9 @@ void Solver::eliminateZ(int j, int k) {
       int nn, pp;
       bool p2p;
     };
+    // a preconditioner that drops every fill-in needs no queue decisions (and
+    // no norm read-back)
+    const bool dropAll = std::isinf(fillInTolerance);
     std::vector<Check> checks;
     for (size_t qn = 0; qn < nbs.size(); ++qn) {
       const int nn = nbs[qn];
@@ -1179,7 +1185,7 @@ void Solver::eliminateZ(int j, int k) {
         else D = E(pp) ? &Bn.M2L[pp] : &Bn.P2L[pp];
         AIFMM_REQUIRE(D->r == Y.r && D->c == T[qp].c, AIFMM_EINVAL, "eliminate_z: fill-in block shape");
         if (Y.c > 0) addg(*D, Y, T[qp], MONE, ONE);
-        if (!E(pp) && wellSeparated(j, nn, pp)) {
+        if (!E(pp) && !dropAll && wellSeparated(j, nn, pp)) {
           if (!E(nn) && nn < pp) checks.push_back({nn, pp, true});
           if (E(nn)) checks.push_back({nn, pp, false});
         }

@@ -23,6 +23,7 @@ struct SolverParams {
   bool phaseTiming = false;              // synchronise at phase boundaries for exact phase times
   bool orthoShortcut = true;             // skip partition 1 of RRQR for orthonormal old bases
   int precision = 0;                     // 1: elimination GEMMs in split TF32 on the tensor cores
+  int drop_pow = 0;                      // fill-in queue threshold 10^-drop_pow (0: 10^-tol_pow; <0: drop all)
 };
 
 struct SolverStats {
@@ -103,6 +104,11 @@ class Solver {
   // that factorize() can run again on the same operator.
   void checkpoint();
   void rewind();
+  // Write the factorized state to a file / replace this solver's state by a
+  // file's (the kernel must have the file's unknown count); a loaded solver
+  // solves without assembling or factorizing.
+  void save(const std::string& path);
+  void load(const std::string& path);
 
  private:
   void createTree();

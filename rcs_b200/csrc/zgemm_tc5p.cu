@@ -473,7 +473,7 @@ long zgemm_tc5p_timeouts() {
   return (long)v;
 }
 
-long tc_timeouts() { return zgemm_tc5_timeouts() + zgemm_tc5p_timeouts(); }
+long tc_timeouts() { return zgemm_tc5_timeouts() + zgemm_tc5p_timeouts() + zgemm_tc6_timeouts(); }
 
 void tc_check(long before, const char* what) {
   const long now = tc_timeouts();

@@ -10,6 +10,7 @@ getAvgMultipoles, findMemory, findMemoryAfterFactorize, nLevels).
 from __future__ import annotations
 
 import ctypes as C
+import os
 
 import numpy as np
 
@@ -47,12 +48,15 @@ class _TreeView:
 class AIFMM:
     def __init__(self, K: kernel, leaf_size: int = 64, tol_pow: int = 8, fillin_tol: int = 10,
                  fillin_rank: int = 0, n_levels: int = 0, precision: int = 0, exact_rrqr: bool = False,
-                 locations=None, domain=None):
+                 locations=None, domain=None, drop_pow: int = 0):
         """locations (N, 3) and domain (xmin, xmax, ymin, ymax, zmin, zmax) play
         the parts of inputsToSolverClass::locations and xmin..zmax; by default
-        the tree is built over the kernel's own unknown locations."""
+        the tree is built over the kernel's own unknown locations.  drop_pow
+        sets the fill-in queue threshold of a factorization used as a
+        preconditioner (0: the reference's 10^-tol_pow; k > 0: 10^-k; negative:
+        every well-separated fill-in is dropped)."""
         p = _lib.SolverParams(int(leaf_size), int(tol_pow), int(fillin_tol), int(fillin_rank), int(n_levels),
-                              int(precision), int(bool(exact_rrqr)))
+                              int(precision), int(bool(exact_rrqr)), int(drop_pow))
         h = C.c_void_p()
         if locations is None and domain is None:
             _lib.check(_lib.lib().aifmm_solver_create(K.h, C.byref(p), C.byref(h)))
@@ -159,6 +163,24 @@ class AIFMM:
     def checkpoint(self) -> None:
         """Keep a device copy of the assembled operator (before factorize)."""
         _lib.check(_lib.lib().aifmm_solver_checkpoint(self.h))
+
+    def save(self, path: str) -> None:
+        """Write the factorization to a checkpoint file (aifmm_solver_save)."""
+        _lib.check(_lib.lib().aifmm_solver_save(self.h, os.fsencode(path)))
+
+    @classmethod
+    def load(cls, K: kernel, path: str) -> "AIFMM":
+        """A solver on kernel K with the factorization read from a checkpoint
+        file (aifmm_solver_load): it solves without assembly or factorization."""
+        self = cls.__new__(cls)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().aifmm_solver_load(K.h, os.fsencode(path), C.byref(h)))
+        self.h = h
+        self.kernel = K
+        self.N = K.N
+        self.A = _TreeView(self)
+        self._rhs = None
+        return self
 
     def rewind(self) -> None:
         """Restore the checkpointed operator so that factorize can run again."""

@@ -2,7 +2,7 @@
 
     python -m rcs_b200.solver_bench [--sub 4] [--radius 0.15] [--freq 2e9] [--leaf 32]
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
-                                    [--precision 0|1|2] [--op-tol 10] [--nrhs 8]
+                                    [--precision 0-4] [--drop-pow 0] [--op-tol 10] [--nrhs 8]
                                     [--gmres 1e-6] [--profile-ops] [--profile-host] [--profile-gemm]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
@@ -33,6 +33,8 @@ def main():
     ap.add_argument("--tol-pow", type=int, default=5)
     ap.add_argument("--fillin-tol", type=int, default=7)
     ap.add_argument("--precision", type=int, default=0)
+    ap.add_argument("--drop-pow", type=int, default=0,
+                    help="fill-in queue threshold 10^-k of the preconditioner (0: the reference's 10^-tol_pow)")
     ap.add_argument("--op-tol", type=int, default=10)
     ap.add_argument("--nrhs", type=int, default=8)
     ap.add_argument("--gmres", type=float, default=None)
@@ -51,7 +53,7 @@ def main():
                   for d in rng.standard_normal((a.nrhs, 3))], axis=1)
     t0 = time.perf_counter()
     S = AIFMM(K, leaf_size=a.leaf, tol_pow=a.tol_pow, fillin_tol=a.fillin_tol, n_levels=a.levels,
-              precision=a.precision)
+              precision=a.precision, drop_pow=a.drop_pow)
     t_asm = time.perf_counter() - t0
     if a.profile_ops:
         S.checkpoint()

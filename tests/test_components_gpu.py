@@ -107,10 +107,10 @@ def test_lu_solve(nrhs):
         assert np.linalg.norm(A @ X - B) / np.linalg.norm(B) < 1e-10
 
 
-@pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6), (2, 2e-6), (3, 2e-6)])
+@pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6), (2, 2e-6), (3, 2e-6), (4, 2e-6)])
 @pytest.mark.parametrize("m,n,k,opA,opB", [
     (64, 64, 16, 0, 0), (1, 1, 1, 0, 0), (65, 33, 17, 1, 0), (200, 130, 451, 0, 1), (37, 300, 5, 1, 1),
-    (10, 10, 0, 0, 0),
+    (10, 10, 0, 0, 0), (300, 260, 1000, 0, 0), (129, 257, 8, 1, 1),
 ])
 def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
     """Grouped GEMM in FP64 and in split TF32 (FP32-level accuracy) against numpy."""
@@ -134,7 +134,7 @@ def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("precision", [2, 3])
+@pytest.mark.parametrize("precision", [2, 3, 4])
 def test_tensor_core_wait_timeout_is_an_error(precision):
     """A tensor-core GEMM whose bounded wait runs out returns AIFMM_ETIMEOUT
     (not a silently unwritten C), and the context stays usable: the wait test

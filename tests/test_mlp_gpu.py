@@ -68,28 +68,38 @@ def _build(ctx, sub, freq, leaf):
 
 
 def test_rank_model_ablation():
-    """Trained on the ACA logs of two spheres, applied to a third (a finer
-    mesh at a higher frequency): identical ranks, fewer reruns of boxes whose
-    rank outgrew the workspace bound, less workspace."""
+    """Trained on the ACA logs of five sphere builds (two meshes, 2-8 GHz),
+    applied to a held-out build inside that range (the finer mesh at 6 GHz,
+    whose ranks, up to about 145, outgrow the fixed 128-term workspace):
+    identical ranks and skeletons (the adaptive ACA decides them), predictions
+    within 25 % (median), and against the fixed bound no reruns of boxes whose
+    rank outgrew the workspace, less workspace and less ACA time."""
     ctx = Context(0)
-    Xa, _, ra, _ = _build(ctx, 4, 4.0e9, 32)
-    Xb, _, rb, _ = _build(ctx, 5, 2.0e9, 128)
+    logs = [_build(ctx, s, f, leaf) for s, f, leaf in
+            ((4, 2.0e9, 64), (4, 6.0e9, 64), (5, 2.0e9, 128), (5, 4.0e9, 128), (5, 8.0e9, 128))]
     m = rankmlp.RankMLP(ctx, seed=3)
-    l0, l1 = m.fit(np.concatenate([Xa, Xb]), np.concatenate([ra, rb]), epochs=3000, lr=3e-3)
-    assert l1 < 0.1 * l0
-    X0, b0, r0, i0 = _build(ctx, 5, 4.0e9, 128)  # fixed bound
+    l0, l1 = m.fit(np.concatenate([x[0] for x in logs]), np.concatenate([x[2] for x in logs]), epochs=3000,
+                   lr=3e-3)
+    assert l1 < 0.05 * l0
+    X0, b0, r0, i0 = _build(ctx, 5, 6.0e9, 128)  # fixed bound
     rankmlp.set_rank_model(ctx, m, 1.25)
     try:
-        X1, b1, r1, i1 = _build(ctx, 5, 4.0e9, 128)  # workspace from the model
+        X1, b1, r1, i1 = _build(ctx, 5, 6.0e9, 128)  # workspace from the model
     finally:
         rankmlp.set_rank_model(ctx, None)
-    assert np.array_equal(r0, r1) and np.array_equal(X0, X1)
+    # the same problems and ranks; a box rerun with a larger bound is logged
+    # when its rerun finishes, so compare the logs in a canonical order
+    def canon(X, r):
+        rows = np.concatenate([X.astype(np.float64), r[:, None].astype(np.float64)], axis=1)
+        return rows[np.lexsort(rows.T[::-1])]
+    assert np.array_equal(canon(X0, r0), canon(X1, r1))
     pred = m.predict_rank(X1)
     rel = np.abs(pred - r1) / np.maximum(r1, 1)
     print("ranks", r1.min(), np.median(r1), r1.max(), "median rel. error", np.median(rel),
           "reruns", i0["n_aca_retry"], "->", i1["n_aca_retry"], "workspace GB", i0["aca_ws_bytes"] / 1e9, "->",
           i1["aca_ws_bytes"] / 1e9, "ACA s", i0["t_aca"], "->", i1["t_aca"])
     assert np.median(rel) < 0.25
-    assert i1["n_aca_retry"] <= i0["n_aca_retry"]
+    assert i0["n_aca_retry"] > 0 and i1["n_aca_retry"] < i0["n_aca_retry"]
     assert i1["aca_ws_bytes"] < i0["aca_ws_bytes"]
+    assert i1["t_aca"] < i0["t_aca"]
     ctx.close()
