@@ -40,21 +40,32 @@ CONFIGS = {
                desc="EFIE PEC sphere R=0.15 m f=1 GHz, 1,280 tri, N=1,920, leaf 64, ACA 1e-8, RRQR 1e-10, "
                     "direct solve"),
     "c3": dict(N=122880, sub=6, radius=0.15, freq=4.0e9, leaf=128, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=9,
-               gmres=1e-6, precision=3,
+               gmres=1e-6, precision=4, drop_pow=2,
                desc="EFIE PEC sphere R=0.15 m f=4 GHz (ka=12.6), 81,920 tri, N=122,880, leaf 128, ACA 1e-5, "
-                    "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 tcgen05 GEMMs over pre-tiled "
-                    "planes) as the preconditioner of FP64 FGMRES(30) to 1e-6 on an ACA-1e-9 H2 operator"),
+                    "RRQR 1e-7, 8 seeded plane waves, mixed factorization (split-TF32 persistent tcgen05 GEMMs; "
+                    "fill-ins under 1e-2 of their M2L block dropped) as the preconditioner of FP64 FGMRES(30) to "
+                    "1e-6 on an ACA-1e-9 H2 operator"),
     "c2": dict(N=81920, kind="es", sub=6, radius=1.0, leaf=128, tol_pow=5, fillin_tol=7, nrhs=33, levels=0,
-               op_tol=10, gmres=1e-8, precision=3,
+               op_tol=10, gmres=1e-8, precision=4,
                desc="Electrostatics unit sphere, 81,920 flat triangles (piecewise-constant charge, collocation at "
                     "centroids), leaf 128, ACA 1e-5, RRQR 1e-7, 32 seeded N(0,1) potentials + the 1 V conductor "
                     "RHS, mixed factorization (split-TF32 tcgen05 GEMMs, FP32-class) as the preconditioner of FP64 "
                     "FGMRES(30) to 1e-8 on an ACA-1e-10 H2 operator; capacitance vs 4 pi eps0 R"),
     "c3s": dict(N=30720, sub=5, radius=0.15, freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=8, levels=0, op_tol=10,
-                gmres=1e-6, precision=3,
+                gmres=1e-6, precision=4, drop_pow=2,
                 desc="EFIE PEC sphere R=0.15 m f=2 GHz, 20,480 tri, N=30,720, leaf 32, ACA 1e-5, RRQR 1e-7, "
                      "8 plane waves, FGMRES(30) to 1e-6 (c3 shape at 1/4 size)"),
 }
+# Batched bodies: 64 seeded ellipsoids (semi-axes U[0.05, 0.3] m), icosphere
+# subdivisions 3 and 4 alternating (1,920 and 7,680 unknowns), 2 GHz, 4 plane
+# waves each; every body on its own context, factorized and refined
+# concurrently (aifmm_batch_factorize / aifmm_batch_solve_gmres).
+BATCH = dict(bodies=64, seed=64, subdivisions=(3, 4), freq=2.0e9, leaf=32, tol_pow=5, fillin_tol=7, nrhs=4,
+             op_tol=10, gmres=1e-6, precision=4, drop_pow=2, threads=16,
+             desc="Batched EFIE: 64 PEC ellipsoids, semi-axes U[0.05,0.3] m (seed 64), icosphere 3/4 alternating "
+                  "(1,920 / 7,680 unknowns), f=2 GHz, 4 plane waves each, leaf 32, ACA 1e-5, RRQR 1e-7; mixed "
+                  "factorization (split-TF32 tcgen05) refined by FP64 FGMRES(30) to 1e-6, bodies on concurrent "
+                  "streams")
 # CPU baseline (reference arm and cpu_baseline): pair updates per timed sample.
 CPU_PAIRS_PER_SAMPLE = 16
 
@@ -177,7 +188,7 @@ def build_workload(cfg, device: int):
         B = np.stack([K.planeWaveRhs(k, e) for k, e in waves], axis=1)
     t0 = time.perf_counter()
     S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"], n_levels=cfg["levels"],
-              precision=cfg.get("precision", 0))
+              precision=cfg.get("precision", 0), drop_pow=cfg.get("drop_pow", 0))
     t_asm = time.perf_counter() - t0
     S.checkpoint()
     A, t_op = None, 0.0
@@ -328,6 +339,11 @@ def run_reference(args, rank, world):
     GPU library.  Rank 0 only."""
     if rank != 0:
         return
+    if args.config not in CONFIGS:
+        print(json.dumps({"impl": "reference", "metric": METRIC, "config": {"workload": args.config},
+                          "unavailable": "the reference arm is measured on the single-geometry configurations "
+                                         "(c1, c2, c3, c3s); the batched one has no CPU run of its own"}), flush=True)
+        return
     cfg = CONFIGS[args.config]
     threads = os.cpu_count() or 1
     t_setup = time.perf_counter()
@@ -358,6 +374,95 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_batch(args, rank, world, local):
+    """The batched-bodies workload: all bodies' factorizations and FGMRES
+    solves per step, concurrently; beside it the same bodies one after another
+    on the plain FP64 path."""
+    import torch
+    from rcs_b200 import batch
+    from rcs_b200.kernel import Context, EFIEMatrix
+    from rcs_b200.solver import AIFMM, H2Operator, launch_count
+    torch.cuda.set_device(local)
+    cfg = BATCH
+    bodies = []
+    t0 = time.perf_counter()
+    for mesh, axes in batch.ellipsoid_family(cfg["bodies"], cfg["seed"], cfg["subdivisions"]):
+        ctx = Context(local)
+        K = EFIEMatrix(mesh, cfg["freq"], ctx=ctx)
+        B = np.stack([K.planeWaveRhs(k, e) for k, e in plane_waves(cfg["nrhs"])], axis=1)
+        S = AIFMM(K, leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"],
+                  precision=cfg["precision"], drop_pow=cfg["drop_pow"])
+        S.checkpoint()
+        A = H2Operator(K, leaf_size=cfg["leaf"], tol_pow=cfg["op_tol"])
+        bodies.append(dict(ctx=ctx, K=K, S=S, A=A, B=B, axes=axes))
+    t_setup = time.perf_counter() - t0
+    Ss, As, Bs = [b["S"] for b in bodies], [b["A"] for b in bodies], [b["B"] for b in bodies]
+    stream = torch.cuda.Stream(device=local)
+    out = {}
+
+    def step():
+        for S in Ss:
+            S.rewind()
+        tf = batch.batch_factorize(Ss, threads=cfg["threads"])
+        xs, recs, ts = batch.batch_solve_gmres(Ss, As, Bs, tol=cfg["gmres"], maxit=300, threads=cfg["threads"])
+        out.update(xs=xs, recs=recs, tf=tf, ts=ts)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    barrier(world)
+    l0 = launch_count()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        torch.cuda.synchronize()
+        e0.record(stream)
+        t_f = t_s = 0.0
+        for _ in range(args.steps):
+            step()  # returns after every body's stream has drained
+            t_f += out["tf"]
+            t_s += out["ts"]
+        e1.record(stream)
+        torch.cuda.synchronize()
+    launches = launch_count() - l0
+    t_step = max_over_ranks(e0.elapsed_time(e1) / 1e3 / args.steps, world)
+    res = [sampled_residual(b["K"], x, b["B"], nrows=256) for b, x in zip(bodies, out["xs"])]
+    # the plain FP64 path, one body after another (one timed pass)
+    plain = None
+    if not args.no_plain:
+        t0 = time.perf_counter()
+        its = []
+        for b in bodies:
+            S0 = AIFMM(b["K"], leaf_size=cfg["leaf"], tol_pow=cfg["tol_pow"], fillin_tol=cfg["fillin_tol"],
+                       precision=0)
+            torch.cuda.synchronize()
+            f0 = time.perf_counter()
+            S0.factorize()
+            _, rec = S0.solve_gmres(b["A"], b["B"], tol=cfg["gmres"], maxit=300)
+            torch.cuda.synchronize()
+            its.append((time.perf_counter() - f0, rec["iterations"]))
+            S0.close()
+        plain = {"value": float(sum(t for t, _ in its)), "unit": "s", "gmres_iterations_mean": float(np.mean(
+            [i for _, i in its])), "mode": "bodies one after another, plain complex128 factorization + FGMRES"}
+    if rank == 0:
+        Ns = [b["K"].N for b in bodies]
+        line = {
+            "metric": METRIC, "value": t_step, "unit": "s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "c128+tf32x3", "data": "synthetic",
+            "config": {"workload": cfg["desc"], "bodies": len(bodies), "N_total": int(sum(Ns)),
+                       "N_min": int(min(Ns)), "N_max": int(max(Ns)), "nrhs": cfg["nrhs"],
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "factor_s": t_f / args.steps, "solve_s": t_s / args.steps,
+            "residual_max": float(max(res)), "residual_per_body": [float(r) for r in res],
+            "gmres_iterations": [r["iterations"] for r in out["recs"]],
+            "plain_fp64": plain, "setup_s": t_setup, "gpu_launches": int(launches), "clocks": clk.summary(),
+            "e2e": {"value": t_step, "unit": "s", "h2d_bytes_per_step": int(16 * sum(Ns) * cfg["nrhs"]),
+                    "d2h_bytes_per_step": int(16 * sum(Ns) * cfg["nrhs"]),
+                    "note": "the batch entry points take host right-hand sides and return host solutions"},
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -375,6 +480,12 @@ def main():
         dist.init_process_group("gloo", timeout=timedelta(seconds=900))
     if args.impl == "reference":
         run_reference(args, rank, world)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+        return
+    if args.config == "c4":
+        run_batch(args, rank, world, local)
         if world > 1:
             import torch.distributed as dist
             dist.destroy_process_group()
@@ -536,7 +647,11 @@ def main():
             "path": ({0: "plain complex128 factorization (reference control flow)",
                       1: "mixed factorization (split-TF32 mma.sync GEMMs)",
                       2: "mixed factorization (split-TF32 tcgen05 GEMMs)",
-                      3: "mixed factorization (split-TF32 tcgen05 GEMMs, pre-tiled planes)"}[cfg.get("precision", 0)]
+                      3: "mixed factorization (split-TF32 tcgen05 GEMMs, pre-tiled planes)",
+                      4: "mixed factorization (split-TF32 persistent warp-specialised tcgen05 GEMMs)"}[
+                         cfg.get("precision", 0)]
+                     + (f", fill-ins under 1e-{cfg['drop_pow']} of their M2L block dropped"
+                        if cfg.get("drop_pow") else "")
                      + (" + FP64 FGMRES" if A is not None else ", direct solve")),
             "residual": res, "residual_e2e": res_e2e, "residual_rows_sampled": min(2048, N),
             "residual_reference": "||Z x - b|| / ||b|| over seeded rows with exact FP64 matrix entries",
@@ -550,8 +665,9 @@ def main():
                      "max_rank": info["max_rank"], "rrqr": info["n_rrqr"]},
             "gpu_launches": int(launches),
             "roofline": {"bound": "tensor",
-                         "kernel": ("zgemm_tc5p_kernel (tcgen05 split-TF32 Schur products; complex-counted "
-                                    "8 m n k flops per product)") if tc else "zgemm_grouped_kernel (FP64)",
+                         "kernel": ((("zgemm_tc6_kernel" if cfg.get("precision") == 4 else "zgemm_tc5p_kernel")
+                                     + " (tcgen05 split-TF32 Schur products; complex-counted 8 m n k flops per "
+                                       "product)") if tc else "zgemm_grouped_kernel (FP64)"),
                          "achieved": dom["tflops"], "peak": dom["peak_tflops"], "unit": "TFLOP/s",
                          "frac": dom["frac"], "peak_source": dom.get("peak", ""),
                          "traffic": None, "launches_profiled": dom["launches"]},

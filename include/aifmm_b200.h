@@ -308,6 +308,22 @@ int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* r
 int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const void* rhs_device, int nrhs,
                                     void* x_device, double tol, int restart, int maxit, aifmm_gmres_info* info);
 
+/* ---- batches of independent bodies (no counterpart call in the reference,
+ * whose driver solves one geometry per process, test/sphere.cpp) ---------- */
+/* Factorizes n solvers concurrently: up to `threads` host threads (<= 0: 16)
+ * each drive one body's AIFMM::factorize() at a time.  Every solver must be
+ * on its own context, so that the bodies' streams overlap on the GPU.  Each
+ * body's result is bit-identical to aifmm_solver_factorize on it alone.
+ * seconds (may be NULL): wall time of the whole batch.  The first failing
+ * body's status is returned; the others still complete. */
+int aifmm_batch_factorize(aifmm_solver* const* solvers, int n, int threads, double* seconds);
+/* FGMRES of every body as aifmm_solver_solve_gmres (host arrays rhs[i], x[i]
+ * of N_i x nrhs[i]), concurrently on the bodies' streams; info: n records
+ * (may be NULL). */
+int aifmm_batch_solve_gmres(aifmm_solver* const* solvers, aifmm_operator* const* ops, const double* const* rhs,
+                            const int* nrhs, double* const* x, int n, double tol, int restart, int maxit, int threads,
+                            aifmm_gmres_info* info, double* seconds);
+
 /* ---- Learned rank prediction (no counterpart in the reference) ----
  * A 6 -> 64 -> 64 -> 1 perceptron (ReLU) with BF16 weights, FP32 activations
  * and FP32 accumulation that predicts log2(1 + rank) of a box's ACA skeleton

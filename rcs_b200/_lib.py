@@ -56,6 +56,9 @@ SIGNATURES = {
     "aifmm_solver_checkpoint": (_i, [_p]),
     "aifmm_solver_rewind": (_i, [_p]),
     "aifmm_solver_save": (_i, [_p, C.c_char_p]),
+    "aifmm_batch_factorize": (_i, [C.POINTER(_p), _i, _i, C.POINTER(_d)]),
+    "aifmm_batch_solve_gmres": (_i, [C.POINTER(_p), C.POINTER(_p), C.POINTER(_p), C.POINTER(_i), C.POINTER(_p), _i,
+                                     _d, _i, _i, _i, _p, C.POINTER(_d)]),
     "aifmm_solver_load": (_i, [_p, C.c_char_p, _pp]),
     "aifmm_launch_count": (_i, [C.POINTER(C.c_long)]),
     "aifmm_tc5_timeouts": (_i, [C.POINTER(C.c_long)]),

@@ -1,9 +1,9 @@
 // Matrix-entry assembly kernels (FP64 reference-exact formulas; the file is
 // compiled with -fmad=false so that a*b+c rounds like the reference) and the
-// host-side construction of the device geometry tables.
+// electrostatic kernel's geometry tables (the EFIE tables are built on the
+// GPU, mesh_build.cu).
 #include <algorithm>
 #include <cmath>
-#include <map>
 #include <vector>
 
 #include "assemble.cuh"
@@ -176,76 +176,6 @@ static void build_tri_table(const double* xyz, int nv, const int* tris, int nt, 
     double l1 = hdist(a, b), l2 = hdist(b, c);
     T[13] = (l2 > l1) ? l2 : l1;
   }
-}
-
-void build_efie_tables(const double* xyz, int nv, const int* tris, int nt, EfieHostTables& h) {
-  build_tri_table(xyz, nv, tris, nt, h.tri);
-  h.node.assign((size_t)(nv + 1) * 4, 0.0);
-  for (int i = 0; i < nv; ++i)
-    for (int q = 0; q < 3; ++q) h.node[(size_t)(i + 1) * 4 + q] = xyz[3 * i + q];
-  // RWG numbering: std::map over (min,max) vertex pairs (EFIEMatrix.cpp:129-209).
-  struct Props {
-    double len;
-    std::vector<int> patches;
-  };
-  std::map<std::pair<int, int>, Props> emap;
-  for (int t = 0; t < nt; ++t) {
-    int id[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
-    for (int e = 0; e < 3; ++e) {
-      int a = id[e], b = id[(e + 1) % 3];
-      auto key = (a < b) ? std::make_pair(a, b) : std::make_pair(b, a);
-      auto it = emap.find(key);
-      if (it == emap.end()) {
-        Props p;
-        p.len = hdist(xyz + 3 * (a - 1), xyz + 3 * (b - 1));
-        p.patches.push_back(t);
-        emap[key] = p;
-      } else {
-        it->second.patches.push_back(t);
-      }
-    }
-  }
-  h.rwg.clear();
-  h.len.clear();
-  h.edge.clear();
-  for (auto& kv : emap) {
-    if (kv.second.patches.size() < 2) continue;
-    const int tp = kv.second.patches[0], tm = kv.second.patches[1];
-    auto third = [&](int t) {  // sorted set difference, EFIEMatrix.cpp:353-373
-      int v[3] = {tris[3 * t], tris[3 * t + 1], tris[3 * t + 2]};
-      std::sort(v, v + 3);
-      int e[2] = {kv.first.first, kv.first.second};
-      std::vector<int> diff(1);
-      std::set_difference(v, v + 3, e, e + 2, diff.begin());
-      return diff[0];
-    };
-    h.rwg.push_back(tp);
-    h.rwg.push_back(tm);
-    h.rwg.push_back(third(tp));
-    h.rwg.push_back(third(tm));
-    h.len.push_back(kv.second.len);
-    h.edge.push_back(kv.first.first);
-    h.edge.push_back(kv.first.second);
-  }
-  const int N = (int)h.len.size();
-  h.side.assign((size_t)N * 2 * SIDE_STRIDE, 0.0);
-  for (int i = 0; i < N; ++i)
-    for (int s = 0; s < 2; ++s) {
-      const int t = h.rwg[4 * i + s], fv = h.rwg[4 * i + 2 + s];
-      const int v1 = tris[3 * t], v2 = tris[3 * t + 1], v3 = tris[3 * t + 2];
-      int i2, i3;  // free vertex first (EFIEMatrix.cpp:480-494)
-      if (v1 == fv) { i2 = v2; i3 = v3; }
-      else if (v2 == fv) { i2 = v1; i3 = v3; }
-      else { i2 = v1; i3 = v2; }
-      double* S = &h.side[((size_t)i * 2 + s) * SIDE_STRIDE];
-      const int ids[3] = {fv, i2, i3};
-      for (int q = 0; q < 3; ++q)
-        for (int c = 0; c < 3; ++c) S[3 * q + c] = xyz[3 * (ids[q] - 1) + c];
-    }
-  h.locations.assign((size_t)N * 3, 0.0);
-  for (int i = 0; i < N; ++i)
-    for (int q = 0; q < 3; ++q)
-      h.locations[3 * i + q] = (xyz[3 * (h.edge[2 * i] - 1) + q] + xyz[3 * (h.edge[2 * i + 1] - 1) + q]) / 2.0;
 }
 
 void build_es_tables(const double* xyz, int nv, const int* tris, int nt, std::vector<double>& tri,

@@ -26,7 +26,15 @@ struct EfieHostTables {
   std::vector<int> rwg, edge;
 };
 
-void build_efie_tables(const double* xyz, int nv, const int* tris, int nt, EfieHostTables& h);
+// EFIE tables of a mesh, built on the GPU (mesh_build.cu): triangle geometry,
+// and the RWG numbering of the reference's std::map over edge keys
+// (src/EFIEMatrix.cpp:129-209) from a stable radix sort of the 3 nt edge keys.
+void build_efie_tables_gpu(aifmm_ctx* ctx, const double* xyz, int nv, const int* tris, int nt, EfieHostTables& h);
+// Octree binning on the GPU (T:576-625): the point indices in leaf order
+// (stable: index order inside a leaf) and leafStart[k]..leafStart[k+1] of
+// leaf k; centers = every box centre of levels 0..nLevels-1, level by level.
+std::vector<int> bin_points_gpu(aifmm_ctx* ctx, const std::vector<double>& pts, const std::vector<double>& centers,
+                                int nLevels, std::vector<int>& leafStart);
 void build_es_tables(const double* xyz, int nv, const int* tris, int nt, std::vector<double>& tri,
                      std::vector<double>& locations);
 

@@ -271,7 +271,7 @@ int aifmm_kernel_create_efie(aifmm_ctx* ctx, const double* nodes, int n_nodes, c
   AIFMM_REQUIRE(freq > 0 && std::isfinite(freq), AIFMM_EINVAL, "frequency must be positive");
   AIFMM_CUDA(cudaSetDevice(ctx->device));
   EfieHostTables h;
-  build_efie_tables(nodes, n_nodes, tris, n_tris, h);
+  build_efie_tables_gpu(ctx, nodes, n_nodes, tris, n_tris, h);
   AIFMM_REQUIRE(!h.len.empty(), AIFMM_EINVAL, "mesh has no RWG (shared) edges");
   std::unique_ptr<aifmm_kernel> k(new aifmm_kernel);
   k->ctx = ctx;

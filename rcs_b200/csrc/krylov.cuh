@@ -22,3 +22,6 @@ struct GmresResult {
 GmresResult fgmres(Solver& M, H2Operator& A, const zd* b, zd* x, int nr, double tol, int restart, int maxit);
 
 }  // namespace aifmm
+
+// the C ABI's record of a solve (include/aifmm_b200.h)
+extern "C" void fill_gmres_info(const aifmm::GmresResult& r, aifmm_gmres_info* info);

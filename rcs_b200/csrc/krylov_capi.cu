@@ -72,7 +72,7 @@ int aifmm_operator_destroy(aifmm_operator* op) {
   API_END
 }
 
-static void fill_info(const GmresResult& r, aifmm_gmres_info* info) {
+void fill_gmres_info(const GmresResult& r, aifmm_gmres_info* info) {
   if (!info) return;
   info->iterations = r.iterations;
   info->cycles = r.cycles;
@@ -91,7 +91,7 @@ int aifmm_solver_solve_gmres_device(aifmm_solver* s, aifmm_operator* A, const vo
   const GmresResult r = fgmres(S, *A->op, static_cast<const zd*>(rhs_device), static_cast<zd*>(x_device), nrhs, tol,
                                restart, maxit);
   AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
-  fill_info(r, info);
+  fill_gmres_info(r, info);
   API_END
 }
 
@@ -108,7 +108,7 @@ int aifmm_solver_solve_gmres(aifmm_solver* s, aifmm_operator* A, const double* r
   const GmresResult r = fgmres(S, *A->op, bd.as<zd>(), xd.as<zd>(), nrhs, tol, restart, maxit);
   AIFMM_CUDA(cudaMemcpyAsync(x, xd.p, bytes, cudaMemcpyDeviceToHost, S.ctx->stream));
   AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
-  fill_info(r, info);
+  fill_gmres_info(r, info);
   API_END
 }
 

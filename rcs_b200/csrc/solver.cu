@@ -139,24 +139,14 @@ void Solver::assignInteractions() {  // T:266-331
       }
 }
 
-void Solver::assignCharges() {  // T:576-668
-  for (int i = 0; i < N; ++i) tree[0][0].chargeLocations.push_back(i);
+void Solver::assignCharges() {  // T:576-668, the binning on the GPU
+  std::vector<double> centers;
   for (int j = 0; j < nLevels; ++j)
-    for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
-      const double* c = tree[j][k].center;
-      for (int index : tree[j][k].chargeLocations) {
-        const double* p = &particles[3 * index];
-        int ch;
-        if (p[2] <= c[2]) {
-          if (p[0] <= c[0]) ch = (p[1] <= c[1]) ? 0 : 3;
-          else ch = (p[1] <= c[1]) ? 1 : 2;
-        } else {
-          if (p[0] <= c[0]) ch = (p[1] <= c[1]) ? 4 : 7;
-          else ch = (p[1] <= c[1]) ? 5 : 6;
-        }
-        tree[j + 1][8 * k + ch].chargeLocations.push_back(index);
-      }
-    }
+    for (int k = 0; k < nBoxesPerLevel[j]; ++k) centers.insert(centers.end(), tree[j][k].center, tree[j][k].center + 3);
+  std::vector<int> start;
+  const std::vector<int> order = bin_points_gpu(ctx, particles, centers, nLevels, start);
+  for (int k = 0; k < nBoxesPerLevel[nLevels]; ++k)
+    tree[nLevels][k].chargeLocations.assign(order.begin() + start[k], order.begin() + start[k + 1]);
   for (int j = nLevels - 1; j >= 0; j--)
     for (int k = 0; k < nBoxesPerLevel[j]; ++k) {
       auto& cl = tree[j][k].chargeLocations;
