@@ -51,6 +51,16 @@ int aifmm_ctx_synchronize(aifmm_ctx* ctx);
 /* The context's CUDA stream (a cudaStream_t), for callers that time or
  * overlap work on it. */
 int aifmm_ctx_stream(aifmm_ctx* ctx, void** stream);
+/* The GEMM autotuner's trials on this context (GEMM precision 5; no
+ * counterpart in the reference): one line per launch class with each
+ * candidate kernel's time and the choice, NUL-terminated into buf (cap
+ * bytes); *len = the report's full length.  The environment variable
+ * AIFMM_TUNE_FILE names a file that stores the choices across runs. */
+int aifmm_ctx_tune_report(aifmm_ctx* ctx, char* buf, int cap, int* len);
+/* Fixes the operand form (0 packed real, 1 split planes: the default) and
+ * tile order (0 row-major: the default, 1 column-major) of GEMM precision 4
+ * on this context, the autotuner's knobs (no counterpart in the reference). */
+int aifmm_ctx_set_gemm_tiling(aifmm_ctx* ctx, int form, int raster);
 
 /* ---- matrix-entry kernels ------------------------------------------------ */
 /* EFIE kernel over a flat-triangle mesh: replaces
@@ -159,7 +169,7 @@ int aifmm_rrqr_noalloc(const void* A_device, int m, int n, int partition, int to
  * tensor-memory accumulators, 3 by tcgen05 over operands split once into
  * pre-tiled planes streamed with bulk copies, 4 by the persistent,
  * warp-specialised tcgen05 kernel over the real form of the complex product
- * (128 x 128 complex tiles).  The dense products of the reference go through Eigen;
+ * (128 x 128 complex tiles), 5 by the autotuner's choice among 3 and 4.  The dense products of the reference go through Eigen;
  * this is the kernel that replaces them on the GPU. */
 int aifmm_zgemm(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double alpha[2],
                 const double* A, int lda, const double* B, int ldb, const double beta[2], double* C, int ldc);
@@ -188,8 +198,10 @@ typedef struct {
                     * 3 = tcgen05 over operands split once into pre-tiled planes;
                     * 4 = the persistent, warp-specialised tcgen05 GEMM over
                     * pre-tiled planes of the real form [Ar Ai][[Br Bi][-Bi Br]]
-                    * (128 x 128 complex tiles, double-buffered accumulators;
-                    * the fastest form) */
+                    * (128 x 128 complex tiles, double-buffered accumulators);
+                    * 5 = the tensor-core kernel and tile order chosen per
+                    * launch class by the library's autotuner (3 or 4; see
+                    * aifmm_ctx_tune_report) */
   int exact_rrqr;  /* 1 = run every recompression RRQR through the full partition-1
                     * Householder pass, as the reference does; 0 (default) skips
                     * that pass when the old basis is one this solver produced with

@@ -32,6 +32,8 @@ SIGNATURES = {
     "aifmm_ctx_destroy": (_i, [_p]),
     "aifmm_ctx_synchronize": (_i, [_p]),
     "aifmm_ctx_stream": (_i, [_p, _pp]),
+    "aifmm_ctx_tune_report": (_i, [_p, C.c_char_p, _i, C.POINTER(_i)]),
+    "aifmm_ctx_set_gemm_tiling": (_i, [_p, _i, _i]),
     "aifmm_kernel_create_efie": (_i, [_p, _dp, _i, _ip, _i, _d, _pp]),
     "aifmm_kernel_create_es": (_i, [_p, _dp, _i, _ip, _p, _i, _pp]),
     "aifmm_kernel_destroy": (_i, [_p]),

@@ -263,6 +263,28 @@ int aifmm_ctx_stream(aifmm_ctx* ctx, void** stream) {
   API_END
 }
 
+int aifmm_ctx_set_gemm_tiling(aifmm_ctx* ctx, int form, int raster) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx && (form == 0 || form == 1) && (raster == 0 || raster == 1), AIFMM_EINVAL,
+                "form and raster must be 0 or 1");
+  ctx->gemmForm = form;
+  ctx->gemmRaster = raster;
+  API_END
+}
+
+int aifmm_ctx_tune_report(aifmm_ctx* ctx, char* buf, int cap, int* len) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx && len, AIFMM_EINVAL, "NULL argument");
+  const std::string r = tune_report(ctx);
+  *len = (int)r.size();
+  if (buf && cap > 0) {
+    const int n = std::min((int)r.size(), cap - 1);
+    std::memcpy(buf, r.data(), (size_t)n);
+    buf[n] = 0;
+  }
+  API_END
+}
+
 int aifmm_kernel_create_efie(aifmm_ctx* ctx, const double* nodes, int n_nodes, const int* tris, int n_tris,
                              double freq, aifmm_kernel** out) {
   API_BEGIN

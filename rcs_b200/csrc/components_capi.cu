@@ -177,7 +177,7 @@ static void zgemm_checked(aifmm_ctx* ctx, int precision, int opA, int opB, int m
 static void zgemm_args(aifmm_ctx* ctx, int precision, int opA, int opB, int m, int n, int k, const double* alpha,
                        const void* A, int lda, const void* B, int ldb, const double* beta, const void* C, int ldc) {
   AIFMM_REQUIRE(ctx && alpha && beta && C && m >= 0 && n >= 0 && k >= 0, AIFMM_EINVAL, "bad argument");
-  AIFMM_REQUIRE(precision >= 0 && precision <= 4, AIFMM_EINVAL, "precision must be 0, 1, 2, 3 or 4");
+  AIFMM_REQUIRE(precision >= 0 && precision <= 5, AIFMM_EINVAL, "precision must be 0 to 5");
   AIFMM_REQUIRE((opA == 0 || opA == 1) && (opB == 0 || opB == 1), AIFMM_EINVAL, "op must be 0 or 1");
   const int ar = opA ? k : m, br = opB ? n : k;
   AIFMM_REQUIRE(lda >= std::max(ar, 1) && ldb >= std::max(br, 1) && ldc >= std::max(m, 1), AIFMM_EINVAL,

@@ -1,6 +1,7 @@
 // Library context: one device, one stream, a stream-ordered device memory
 // pool, and the kernel (mesh) objects.
 #pragma once
+#include <map>
 #include <memory>
 #include <mutex>
 #include <string>
@@ -20,6 +21,14 @@ struct aifmm_ctx {
   cudaMemPool_t pool = nullptr;
   size_t bytes_live = 0;
   int refs = 1;          // the creator's reference
+  int gemmRaster = 0;    // tile order of the persistent tensor-core GEMM (set by the autotuner)
+  bool splitK = true;    // FP64 launches with few output tiles and long depths split their depth
+  int gemmForm = 1;      // operand form of the persistent tensor-core GEMM: 0 packed real, 1 split planes
+                         // (the default: 32 instead of 48 KB per 8-deep step; faster on the solver's products)
+  // Autotuner choices of the tensor-core GEMM by launch class (autotune.cu)
+  std::mutex tuneMu;
+  std::map<long long, int> tuneCache;
+  std::vector<std::string> tuneLog;
   int gemmPrecision = 0; // grouped GEMMs: 0 complex128 FMA; split TF32 (FP32 accuracy) on the tensor
                          // cores: 1 mma.sync, 2 tcgen05 with tensor-memory accumulators
   // Pinned staging ring for the small host-to-device uploads (problem lists,

@@ -514,13 +514,156 @@ static void zgemm_skinny_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>&
   AIFMM_LAUNCHED();
 }
 
+static void zgemm_chained_dispatch(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs,
+                                   const std::vector<int>& chain);
+
+// ---- split-K for FP64 launches with few output tiles and long depths
+// (the Gram-Schmidt projections Q^H F of the recompressions: a few dozen
+// 64 x 64 tiles over depths of 500-2,000).  Every chain's depth is cut into S
+// ranges that become separate chains writing partial sums into a workspace;
+// a second kernel adds the partials in a fixed order (deterministic) and
+// applies alpha and beta.
+struct SplitOut {
+  zd* C;
+  int m, n, ldc, parts;
+  zd alpha, beta;
+  long part0;  // first element of this chain's partials in the workspace
+};
+
+__global__ void zsplitk_reduce_kernel(const SplitOut* __restrict__ outs, const long* __restrict__ start, int nouts,
+                                      long total, const zd* __restrict__ work) {
+  for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
+    int lo = 0, hi = nouts - 1;
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (start[mid] <= t) lo = mid;
+      else hi = mid - 1;
+    }
+    const SplitOut& O = outs[lo];
+    const long u = t - start[lo];
+    const int r = (int)(u % O.m), c = (int)(u / O.m);
+    const long mn = (long)O.m * O.n;
+    zd acc = work[O.part0 + u];
+    for (int s = 1; s < O.parts; ++s) acc = zadd(acc, work[O.part0 + (long)s * mn + u]);
+    zd* cp = O.C + (size_t)c * O.ldc + r;
+    zd v = zmul(O.alpha, acc);
+    if (O.beta.x != 0.0 || O.beta.y != 0.0) v = zadd(v, zmul(O.beta, *cp));
+    *cp = v;
+  }
+}
+
+// true when the FP64 launch fills under a third of the SMs with long depths
+static bool splitk_wanted(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
+  long tiles = 0, depth = 0, chains = 0;
+  for (size_t i = 0; i < probs.size();) {
+    const GemmProblem& h = probs[i];
+    long k = 0;
+    for (int q = 0; q < chain[i]; ++q) k += std::max(probs[i + q].k, 0);
+    if (h.m > 0 && h.n > 0) {
+      tiles += (long)((h.m + GBM - 1) / GBM) * ((h.n + GBN - 1) / GBN);
+      depth = std::max(depth, k);
+      chains++;
+    }
+    i += chain[i];
+  }
+  const int sms = ctx->numSMs > 0 ? ctx->numSMs : 148;
+  return chains > 0 && tiles * 3 <= sms && depth >= 384;
+}
+
+static void zgemm_splitk(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
+  const int sms = ctx->numSMs > 0 ? ctx->numSMs : 148;
+  long tiles = 0;
+  for (size_t i = 0; i < probs.size(); i += chain[i])
+    if (probs[i].m > 0 && probs[i].n > 0)
+      tiles += (long)((probs[i].m + GBM - 1) / GBM) * ((probs[i].n + GBN - 1) / GBN);
+  const int S = (int)std::max(2L, std::min(16L, (2L * sms + tiles - 1) / std::max(tiles, 1L)));
+  std::vector<GemmProblem> ps;
+  std::vector<int> ch;
+  std::vector<long> woff;  // workspace offset of each piece's partial
+  std::vector<SplitOut> outs;
+  long work = 0;
+  for (size_t i = 0; i < probs.size(); i += chain[i]) {
+    const GemmProblem& h = probs[i];
+    if (h.m <= 0 || h.n <= 0) continue;
+    long K = 0;
+    for (int q = 0; q < chain[i]; ++q) K += std::max(probs[i + q].k, 0);
+    const int parts = (int)std::max(1L, std::min((long)S, K / 128));
+    const long kc = (K + parts - 1) / parts;
+    const long mn = (long)h.m * h.n;
+    outs.push_back({h.C, h.m, h.n, h.ldc, parts, h.alpha, h.beta, work});
+    for (int s = 0; s < parts; ++s) {
+      const long lo = s * kc, hi = std::min(K, lo + kc);
+      // the pieces of the chain's problems that fall in [lo, hi)
+      std::vector<GemmProblem> piece;
+      long base = 0;
+      for (int q = 0; q < chain[i]; ++q) {
+        const GemmProblem& p = probs[i + q];
+        const long a = std::max(lo, base), b = std::min(hi, base + std::max(p.k, 0));
+        if (a < b) {
+          GemmProblem x = p;
+          const long k0 = a - base;
+          x.k = (int)(b - a);
+          x.A = (p.opA == OP_N) ? p.A + k0 * p.lda : p.A + k0;
+          x.B = (p.opB == OP_N) ? p.B + k0 : p.B + k0 * p.ldb;
+          piece.push_back(x);
+        }
+        base += std::max(p.k, 0);
+      }
+      if (piece.empty()) {  // an empty range: a zero product keeps the partial defined
+        GemmProblem x = h;
+        x.k = 0;
+        piece.push_back(x);
+      }
+      for (size_t q = 0; q < piece.size(); ++q) {
+        GemmProblem x = piece[q];
+        x.C = nullptr;  // set below, once the workspace exists
+        x.ldc = h.m;
+        x.alpha = zmk(1, 0);
+        x.beta = q == 0 ? zmk(0, 0) : zmk(1, 0);
+        woff.push_back(work + s * mn);
+        ps.push_back(x);
+        ch.push_back(q == 0 ? (int)piece.size() : 0);
+      }
+    }
+    work += (long)parts * mn;
+  }
+  DevBuf ws(ctx, sizeof(zd) * std::max(work, 1L));
+  for (size_t q = 0; q < ps.size(); ++q) ps[q].C = ws.as<zd>() + woff[q];
+  zgemm_chained_dispatch(ctx, ps, ch);
+  std::vector<long> start;
+  long total = 0;
+  for (const SplitOut& o : outs) {
+    start.push_back(total);
+    total += (long)o.m * o.n;
+  }
+  DevBuf dout = upload(ctx, outs), dst = upload(ctx, start);
+  const int grid = (int)std::min<long>((total + 255) / 256, 148L * 16);
+  zsplitk_reduce_kernel<<<grid, 256, 0, ctx->stream>>>(dout.as<SplitOut>(), dst.as<long>(), (int)outs.size(), total,
+                                                       ws.as<zd>());
+  AIFMM_LAUNCHED();
+}
+
 void zgemm_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain) {
   AIFMM_REQUIRE(probs.size() == chain.size(), AIFMM_EINVAL, "chain lengths do not match the problems");
+  if (ctx->gemmPrecision == 0 && ctx->splitK && !skinny_eligible(probs) && splitk_wanted(ctx, probs, chain)) {
+    zgemm_splitk(ctx, probs, chain);
+    return;
+  }
+  zgemm_chained_dispatch(ctx, probs, chain);
+}
+
+// One launch of the kernel the context's GEMM precision selects.
+static void zgemm_chained_dispatch(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs,
+                                   const std::vector<int>& chain) {
   std::vector<GemmProblem> ps;
   std::vector<GemmGroup> gs;
   long tiles = 0;
   double flops = 0;
   const int mode = ctx->gemmPrecision;
+  if (mode == 5) {
+    zgemm_tuned(ctx, probs, chain);
+    return;
+  }
   const int bm = (mode >= 2) ? 128 : GBM;  // row tile of the tcgen05 kernels
   const int bn = (mode == 4) ? 128 : GBN;  // complex columns per tile
   for (size_t i = 0; i < probs.size();) {

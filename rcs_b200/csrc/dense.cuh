@@ -44,6 +44,9 @@ struct GemmArgs {
   // that nothing sets, so that the wait runs out)
   unsigned long long waitNs;
   const int* hold;
+  // persistent tensor-core GEMM: tile order inside a group (0: row-major,
+  // 1: column-major), picked by the autotuner
+  int raster;
   GemmProblem ip[GEMM_INLINE];
   GemmGroup ig[GEMM_INLINE];
 };
@@ -71,6 +74,10 @@ void zgemm_tc5p(aifmm_ctx* ctx, std::vector<GemmProblem> ps, const std::vector<G
 // tilesN = ceil(n / 128) and ceil(m / 128) row tiles.
 long zgemm_tc6_timeouts();
 void zgemm_tc6(aifmm_ctx* ctx, const std::vector<GemmProblem>& ps, const std::vector<GemmGroup>& gs);
+// GEMM precision 5: the tensor-core kernel and tile order picked per launch
+// class by the autotuner (autotune.cu); tune_report lists its trials.
+void zgemm_tuned(aifmm_ctx* ctx, const std::vector<GemmProblem>& probs, const std::vector<int>& chain);
+std::string tune_report(aifmm_ctx* ctx);
 
 // C = alpha op(A) op(B) + beta C for every problem, one launch; the
 // problems must write disjoint C.

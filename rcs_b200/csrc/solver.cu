@@ -1233,6 +1233,12 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   AIFMM_CUDA(cudaSetDevice(ctx->device));
   const long tc0 = prm.precision >= 2 ? tc_timeouts() : 0;
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
+  // A fresh tree's fill-in queues are empty.  The reference does not clear
+  // them between levels, and pairs queued late at one level can still be
+  // waiting when its elimination ends; a refactorization after rewind() must
+  // not inherit them from the previous factorization.
+  P2Pq.clear();
+  P2L_M2P.clear();
   stats.flops_factor = 0;
   baseLU_ = DLU();
   baseReady_ = false;

@@ -15,8 +15,8 @@ extern "C" {
 static void solver_create(aifmm_kernel* k, const aifmm_solver_params* p, const double* xyz, const double* dom,
                           aifmm_solver** out) {
   AIFMM_REQUIRE(k && p && out, AIFMM_EINVAL, "NULL argument");
-  AIFMM_REQUIRE(p->precision >= 0 && p->precision <= 4, AIFMM_EINVAL,
-                "precision must be 0 (plain), 1, 2, 3 or 4 (mixed)");
+  AIFMM_REQUIRE(p->precision >= 0 && p->precision <= 5, AIFMM_EINVAL,
+                "precision must be 0 (plain) or 1 to 5 (mixed)");
   AIFMM_REQUIRE(p->leaf_size > 0 && p->tol_pow >= 0 && p->fillin_tol >= 0 && p->n_levels >= 0, AIFMM_EINVAL,
                 "bad solver parameters");
   SolverParams sp;

@@ -34,6 +34,19 @@
 // test); a wait that runs out makes the CTA stop, drain what it has in
 // flight, leave its remaining tiles unwritten and count the failure
 // (zgemm_tc6_timeouts()).
+//
+// A second operand form (FORM 1, "split planes") keeps the real and imaginary
+// parts apart instead: A as four planes (Ar hi, Ar lo, Ai hi, Ai lo) of
+// 128 rows, B likewise with 128 rows, and per 8-deep complex step twelve
+// 128x128x8 MMAs into two accumulators, Cr += Ar Br - Ai Bi (the minus by the
+// instruction's B negation) and Ci += Ar Bi + Ai Br, each as hi*hi + hi*lo +
+// lo*hi.  The MMA work is the same; the operand bytes per step drop from 48 KB
+// to 32 KB because B is not stored twice, at the price of twice as many
+// (half as wide) MMAs.  The ring then holds six 32 KB stages.  On the
+// solver's Schur launches (products of 100-1,000 on a side) the split form is
+// 5-15 % faster and is the default (aifmm_ctx_set_gemm_tiling, the autotuner
+// of GEMM precision 5 picks per launch class); on large square products the
+// packed form's wider MMAs win.
 #include <algorithm>
 #include <map>
 
@@ -41,18 +54,28 @@
 
 namespace aifmm {
 
-constexpr int T6_M = 128, T6_NC = 128, T6_N = 2 * T6_NC, T6_KS = 16, T6_STAGES = 4, T6_THREADS = 192;
+constexpr int T6_M = 128, T6_NC = 128, T6_N = 2 * T6_NC, T6_KS = 16, T6_THREADS = 192;
 constexpr uint32_t T6_TMEM_COLS = 512;
 constexpr uint32_t T6_A_WORDS = 2 * 2 * T6_M * 8, T6_B_WORDS = 2 * 2 * T6_N * 8;  // per slice chunk
-constexpr uint32_t T6_A_BYTES = T6_A_WORDS * 4, T6_B_BYTES = T6_B_WORDS * 4;      // 16 KB, 32 KB
 
-struct T6Stage {
-  uint32_t A[2][2][T6_M * 8];  // [hi/lo][k-step][core-matrix layout]
-  uint32_t B[2][2][T6_N * 8];
+// per-form chunk sizes (32-bit words) and ring depth
+template <int FORM>
+struct T6Form;
+template <>
+struct T6Form<0> {  // packed real: A [hi/lo][k-step][128 x 8], B [hi/lo][k-step][256 x 8]
+  static constexpr uint32_t A_WORDS = T6_A_WORDS, B_WORDS = T6_B_WORDS;
+  static constexpr int STAGES = 4;
 };
+template <>
+struct T6Form<1> {  // split planes: A [re hi, re lo, im hi, im lo][128 x 8], B the same
+  static constexpr uint32_t A_WORDS = 4 * T6_M * 8, B_WORDS = 4 * T6_NC * 8;
+  static constexpr int STAGES = 6;
+};
+template <int FORM>
 struct T6Smem {
-  T6Stage st[T6_STAGES];
-  unsigned long long full[T6_STAGES], empty[T6_STAGES], accFull[2], accEmpty[2];
+  static constexpr uint32_t STAGE_WORDS = T6Form<FORM>::A_WORDS + T6Form<FORM>::B_WORDS;
+  uint32_t ring[T6Form<FORM>::STAGES][STAGE_WORDS];  // each stage: A chunk, then B chunk
+  unsigned long long full[T6Form<FORM>::STAGES], empty[T6Form<FORM>::STAGES], accFull[2], accEmpty[2];
   uint32_t tmem_slot;
   int err;
 };
@@ -73,14 +96,18 @@ __device__ __forceinline__ uint64_t t6_desc(const void* p) {
   return d;
 }
 // kind::tf32, FP32 accumulator, both operands K-major, M = 128, N = 256
+// (packed real) or N = 128 with and without B negated (split planes)
 constexpr uint32_t T6_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(T6_N >> 3) << 17) |
                               ((uint32_t)(T6_M >> 4) << 24);
+constexpr uint32_t T6_IDESC_S = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(T6_NC >> 3) << 17) |
+                                ((uint32_t)(T6_M >> 4) << 24);
+constexpr uint32_t T6_IDESC_SN = T6_IDESC_S | (1u << 14);
 
-__device__ __forceinline__ void t6_mma(uint32_t d, uint64_t da, uint64_t db, uint32_t acc) {
+__device__ __forceinline__ void t6_mma(uint32_t d, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
   asm volatile(
       "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
       "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-      "l"(da), "l"(db), "r"(T6_IDESC), "r"(acc));
+      "l"(da), "l"(db), "r"(idesc), "r"(acc));
 }
 __device__ __forceinline__ void t6_commit(unsigned long long* bar) {
   asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(t6_smem(bar))
@@ -122,6 +149,7 @@ struct T6Operand {
   uint32_t* dst;
   int rows, k, ld, op, isB;  // rows: M of op(A) / N of op(B); k: complex depth
   int nks;                   // slices (8 complex k each)
+  int form;                  // 0 packed real, 1 split planes
 };
 
 __device__ __forceinline__ uint32_t t6_tf32(float x) {
@@ -129,13 +157,23 @@ __device__ __forceinline__ uint32_t t6_tf32(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return r;
 }
-__device__ __forceinline__ void t6_put(uint32_t* chunk, int planeWords, int off, float x) {
-  const uint32_t h = t6_tf32(x);
-  chunk[off] = h;
-  chunk[planeWords + off] = t6_tf32(x - __uint_as_float(h));
+
+__device__ __forceinline__ void t6_split4(const float (&x)[4], uint4& hi, uint4& lo) {
+  uint32_t h[4], l[4];
+#pragma unroll
+  for (int q = 0; q < 4; ++q) {
+    h[q] = t6_tf32(x[q]);
+    l[q] = t6_tf32(x[q] - __uint_as_float(h[q]));
+  }
+  hi = make_uint4(h[0], h[1], h[2], h[3]);
+  lo = make_uint4(l[0], l[1], l[2], l[3]);
 }
 
-// One thread per padded complex element (row, k) of every operand.
+// One thread per (padded row, four consecutive complex k) of every operand:
+// it reads the four entries and writes them as 16-byte vectors (the core
+// matrix layout keeps four consecutive depths of a row together), so a warp's
+// stores cover whole 128-byte lines.  Consecutive threads take consecutive
+// rows.
 __global__ void t6_convert_kernel(const T6Operand* __restrict__ ops, const long* __restrict__ start, int nops,
                                   long total) {
   for (long t = blockIdx.x * (long)blockDim.x + threadIdx.x; t < total; t += (long)gridDim.x * blockDim.x) {
@@ -148,38 +186,66 @@ __global__ void t6_convert_kernel(const T6Operand* __restrict__ ops, const long*
     const T6Operand& O = ops[lo];
     const long u = t - start[lo];
     const int tileRows = O.isB ? T6_NC : T6_M;
-    const int prow = ((O.rows + tileRows - 1) / tileRows) * tileRows, pk = O.nks * 8;
-    // walk the contiguous dimension of the source with consecutive threads
-    const bool rowFast = O.isB ? (O.op == OP_C) : (O.op == OP_N);
-    int r, k;
-    if (rowFast) {
-      r = (int)(u % prow);
-      k = (int)(u / prow);
-    } else {
-      k = (int)(u % pk);
-      r = (int)(u / pk);
-    }
-    zd v = zmk(0, 0);
-    if (r < O.rows && k < O.k) {
-      if (!O.isB) v = (O.op == OP_N) ? O.src[(size_t)k * O.ld + r] : zconj(O.src[(size_t)r * O.ld + k]);
-      else v = (O.op == OP_N) ? O.src[(size_t)r * O.ld + k] : zconj(O.src[(size_t)k * O.ld + r]);
+    const int prow = ((O.rows + tileRows - 1) / tileRows) * tileRows;
+    const int r = (int)(u % prow), q = (int)(u / prow);  // row, quad of complex depths 4q..4q+3
+    float re[4], im[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int k = 4 * q + i;
+      zd v = zmk(0, 0);
+      if (r < O.rows && k < O.k) {
+        if (!O.isB) v = (O.op == OP_N) ? O.src[(size_t)k * O.ld + r] : zconj(O.src[(size_t)r * O.ld + k]);
+        else v = (O.op == OP_N) ? O.src[(size_t)r * O.ld + k] : zconj(O.src[(size_t)k * O.ld + r]);
+      }
+      re[i] = (float)v.x;
+      im[i] = (float)v.y;
     }
     const int tr = r / tileRows, rr = r % tileRows;
-    const int d = 2 * k, ks = d / T6_KS, dd = d % T6_KS, step = dd >> 3, kk = dd & 7;  // kk even: kk+1 in step
-    const float re = (float)v.x, im = (float)v.y;
+    const int rowOff = (rr >> 3) * 64 + (rr & 7) * 4;
+    uint4 h, l;
+    if (O.form == 1) {  // planes re hi, re lo, im hi, im lo; slice = 8 complex k
+      const int ks = q >> 1, half = q & 1;
+      const uint32_t words = O.isB ? T6Form<1>::B_WORDS : T6Form<1>::A_WORDS;
+      uint32_t* c = O.dst + ((size_t)tr * O.nks + ks) * words + rowOff + half * 32;
+      t6_split4(re, h, l);
+      *reinterpret_cast<uint4*>(c) = h;
+      *reinterpret_cast<uint4*>(c + 1024) = l;
+      t6_split4(im, h, l);
+      *reinterpret_cast<uint4*>(c + 2048) = h;
+      *reinterpret_cast<uint4*>(c + 3072) = l;
+      continue;
+    }
+    // packed real: real depths 8q..8q+7 = one k-step of the slice q / 2
+    const int ks = q >> 1, step = q & 1;
     if (!O.isB) {
-      uint32_t* c = O.dst + ((size_t)tr * O.nks + ks) * T6_A_WORDS + (size_t)step * (T6_M * 8);
+      uint32_t* c = O.dst + ((size_t)tr * O.nks + ks) * T6_A_WORDS + (size_t)step * (T6_M * 8) + rowOff;
       const int pw = 2 * T6_M * 8;  // hi plane -> lo plane
-      t6_put(c, pw, t6_off(rr, kk), re);
-      t6_put(c, pw, t6_off(rr, kk + 1), im);
+      const float a0[4] = {re[0], im[0], re[1], im[1]}, a1[4] = {re[2], im[2], re[3], im[3]};
+      t6_split4(a0, h, l);
+      *reinterpret_cast<uint4*>(c) = h;
+      *reinterpret_cast<uint4*>(c + pw) = l;
+      t6_split4(a1, h, l);
+      *reinterpret_cast<uint4*>(c + 32) = h;
+      *reinterpret_cast<uint4*>(c + pw + 32) = l;
     } else {
       uint32_t* c = O.dst + ((size_t)tr * O.nks + ks) * T6_B_WORDS + (size_t)step * (T6_N * 8);
       const int pw = 2 * T6_N * 8;
       // rows rr (Cr): [Br, -Bi]; rows 128 + rr (Ci): [Bi, Br] along the depth
-      t6_put(c, pw, t6_off(rr, kk), re);
-      t6_put(c, pw, t6_off(rr, kk + 1), -im);
-      t6_put(c, pw, t6_off(T6_NC + rr, kk), im);
-      t6_put(c, pw, t6_off(T6_NC + rr, kk + 1), re);
+      const int offR = rowOff, offI = ((T6_NC + rr) >> 3) * 64 + (rr & 7) * 4;
+      const float r0[4] = {re[0], -im[0], re[1], -im[1]}, r1[4] = {re[2], -im[2], re[3], -im[3]};
+      const float i0[4] = {im[0], re[0], im[1], re[1]}, i1[4] = {im[2], re[2], im[3], re[3]};
+      t6_split4(r0, h, l);
+      *reinterpret_cast<uint4*>(c + offR) = h;
+      *reinterpret_cast<uint4*>(c + pw + offR) = l;
+      t6_split4(r1, h, l);
+      *reinterpret_cast<uint4*>(c + offR + 32) = h;
+      *reinterpret_cast<uint4*>(c + pw + offR + 32) = l;
+      t6_split4(i0, h, l);
+      *reinterpret_cast<uint4*>(c + offI) = h;
+      *reinterpret_cast<uint4*>(c + pw + offI) = l;
+      t6_split4(i1, h, l);
+      *reinterpret_cast<uint4*>(c + offI + 32) = h;
+      *reinterpret_cast<uint4*>(c + pw + offI + 32) = l;
     }
   }
 }
@@ -194,16 +260,33 @@ __device__ __forceinline__ int t6_group(const GemmGroup* G, int ngroups, int til
   }
   return lo;
 }
+// tile -> (row tile, column tile) of its group, in the launch's raster order
+__device__ __forceinline__ void t6_coords(const GemmProblem* probs, const GemmGroup& g, int raster, int tile,
+                                          int& tm, int& tn) {
+  const int local = tile - g.tileStart;
+  if (raster == 0) {
+    tm = local / g.tilesN;
+    tn = local % g.tilesN;
+  } else {
+    const int tilesM = (probs[g.head].m + T6_M - 1) / T6_M;
+    tn = local / tilesM;
+    tm = local % tilesM;
+  }
+}
 __device__ __forceinline__ int t6_slices(const GemmProblem* probs, const GemmGroup& g) {
   int total = 0;
   for (int q = 0; q < g.nchain; ++q) total += (probs[g.head + q].k + 7) / 8;
   return total;
 }
 
-template <bool INLINE>
+template <int FORM, bool INLINE>
 __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_constant__ GemmArgs a, int nTiles) {
+  using F = T6Form<FORM>;
+  constexpr int STAGES = F::STAGES;
+  constexpr uint32_t A_WORDS = F::A_WORDS, B_WORDS = F::B_WORDS;
   extern __shared__ unsigned char t6_raw[];
-  T6Smem& S = *reinterpret_cast<T6Smem*>((reinterpret_cast<uintptr_t>(t6_raw) + 1023) & ~uintptr_t(1023));
+  T6Smem<FORM>& S =
+      *reinterpret_cast<T6Smem<FORM>*>((reinterpret_cast<uintptr_t>(t6_raw) + 1023) & ~uintptr_t(1023));
   const GemmGroup* G = INLINE ? a.ig : a.groups;
   const GemmProblem* probs = INLINE ? a.ip : a.probs;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -216,7 +299,7 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
   }
   if (tid == 32) {
-    for (int s = 0; s < T6_STAGES; ++s) {
+    for (int s = 0; s < STAGES; ++s) {
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t6_smem(&S.full[s])) : "memory");
       asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(t6_smem(&S.empty[s])) : "memory");
     }
@@ -238,41 +321,42 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
       uint32_t it = 0;
       for (int tile = blockIdx.x; tile < nTiles && ok; tile += gridDim.x) {
         const GemmGroup g = G[t6_group(G, a.ngroups, tile)];
-        const int local = tile - g.tileStart, tm = local / g.tilesN, tn = local % g.tilesN;
+        int tm, tn;
+        t6_coords(probs, g, a.raster, tile, tm, tn);
         for (int q = 0; q < g.nchain && ok; ++q) {
           const GemmProblem& P = probs[g.head + q];
           const int nks = (P.k + 7) / 8;
           for (int ks = 0; ks < nks; ++ks, ++it) {
-            const int s = it % T6_STAGES;
-            const uint32_t ph = (it / T6_STAGES) & 1u;
+            const int s = it % STAGES;
+            const uint32_t ph = (it / STAGES) & 1u;
             if (!t6_wait(&S.empty[s], ph ^ 1u, lim) || *(volatile int*)&S.err) {
               ok = false;
               break;
             }
-            const uint32_t* ga = P.pa + ((size_t)tm * nks + ks) * T6_A_WORDS;
-            const uint32_t* gb = P.pb + ((size_t)tn * nks + ks) * T6_B_WORDS;
+            const uint32_t* ga = P.pa + ((size_t)tm * nks + ks) * A_WORDS;
+            const uint32_t* gb = P.pb + ((size_t)tn * nks + ks) * B_WORDS;
             asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(t6_smem(&S.full[s])),
-                         "r"(T6_A_BYTES + T6_B_BYTES)
+                         "r"((A_WORDS + B_WORDS) * 4)
                          : "memory");
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    t6_smem(&S.st[s].A[0][0][0])),
-                "l"(ga), "r"(T6_A_BYTES), "r"(t6_smem(&S.full[s]))
+                    t6_smem(&S.ring[s][0])),
+                "l"(ga), "r"(A_WORDS * 4), "r"(t6_smem(&S.full[s]))
                 : "memory");
             asm volatile(
                 "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                    t6_smem(&S.st[s].B[0][0][0])),
-                "l"(gb), "r"(T6_B_BYTES), "r"(t6_smem(&S.full[s]))
+                    t6_smem(&S.ring[s][A_WORDS])),
+                "l"(gb), "r"(B_WORDS * 4), "r"(t6_smem(&S.full[s]))
                 : "memory");
           }
         }
       }
       if (!ok) S.err = 1;
       // drain: every slot's last copy has landed before the CTA may exit
-      for (int q = 0; q < T6_STAGES && it > 0; ++q) {
+      for (int q = 0; q < STAGES && it > 0; ++q) {
         const int back = (int)it - 1 - q;
         if (back < 0) break;
-        t6_wait(&S.full[back % T6_STAGES], (uint32_t)(back / T6_STAGES) & 1u, lim);
+        t6_wait(&S.full[back % STAGES], (uint32_t)(back / STAGES) & 1u, lim);
       }
     }
   } else if (warp == 1) {
@@ -294,21 +378,43 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
         const GemmGroup g = G[t6_group(G, a.ngroups, tile)];
         const int total = t6_slices(probs, g);
         for (int j = 0; j < total; ++j, ++it) {
-          const int s = it % T6_STAGES;
-          const uint32_t ph = (it / T6_STAGES) & 1u;
+          const int s = it % STAGES;
+          const uint32_t ph = (it / STAGES) & 1u;
           if (!t6_wait(&S.full[s], ph, lim)) {
             ok = false;
             break;
           }
           asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-          T6Stage& st = S.st[s];
+          const uint32_t* sa = &S.ring[s][0];
+          const uint32_t* sb = &S.ring[s][A_WORDS];
+          if (FORM == 0) {
 #pragma unroll
-          for (int step = 0; step < 2; ++step) {
-            const uint64_t ah = t6_desc(st.A[0][step]), al = t6_desc(st.A[1][step]);
-            const uint64_t bh = t6_desc(st.B[0][step]), bl = t6_desc(st.B[1][step]);
-            t6_mma(d, ah, bh, (j | step) ? 1u : 0u);
-            t6_mma(d, ah, bl, 1u);
-            t6_mma(d, al, bh, 1u);
+            for (int step = 0; step < 2; ++step) {  // [plane][step][rows x 8]
+              const uint64_t ah = t6_desc(sa + step * T6_M * 8), al = t6_desc(sa + (2 + step) * T6_M * 8);
+              const uint64_t bh = t6_desc(sb + step * T6_N * 8), bl = t6_desc(sb + (2 + step) * T6_N * 8);
+              t6_mma(d, ah, bh, T6_IDESC, (j | step) ? 1u : 0u);
+              t6_mma(d, ah, bl, T6_IDESC, 1u);
+              t6_mma(d, al, bh, T6_IDESC, 1u);
+            }
+          } else {  // [re hi, re lo, im hi, im lo][128 x 8]
+            const uint64_t arh = t6_desc(sa), arl = t6_desc(sa + 1024), aih = t6_desc(sa + 2048),
+                           ail = t6_desc(sa + 3072);
+            const uint64_t brh = t6_desc(sb), brl = t6_desc(sb + 1024), bih = t6_desc(sb + 2048),
+                           bil = t6_desc(sb + 3072);
+            const uint32_t first = j ? 1u : 0u, dr = d, di = d + T6_NC;
+            // Cr += Ar Br - Ai Bi ; Ci += Ar Bi + Ai Br (hi*hi + hi*lo + lo*hi each)
+            t6_mma(dr, arh, brh, T6_IDESC_S, first);
+            t6_mma(dr, arh, brl, T6_IDESC_S, 1u);
+            t6_mma(dr, arl, brh, T6_IDESC_S, 1u);
+            t6_mma(dr, aih, bih, T6_IDESC_SN, 1u);
+            t6_mma(dr, aih, bil, T6_IDESC_SN, 1u);
+            t6_mma(dr, ail, bih, T6_IDESC_SN, 1u);
+            t6_mma(di, arh, bih, T6_IDESC_S, first);
+            t6_mma(di, arh, bil, T6_IDESC_S, 1u);
+            t6_mma(di, arl, bih, T6_IDESC_S, 1u);
+            t6_mma(di, aih, brh, T6_IDESC_S, 1u);
+            t6_mma(di, aih, brl, T6_IDESC_S, 1u);
+            t6_mma(di, ail, brh, T6_IDESC_S, 1u);
           }
           t6_commit(&S.empty[s]);
           lastSlot = s;
@@ -335,7 +441,8 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
       }
       asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
       const GemmGroup g = G[t6_group(G, a.ngroups, tile)];
-      const int loc = tile - g.tileStart, tm = loc / g.tilesN, tn = loc % g.tilesN;
+      int tm, tn;
+      t6_coords(probs, g, a.raster, tile, tm, tn);
       const GemmProblem& P = probs[g.head];
       const bool any = t6_slices(probs, g) > 0;
       const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
@@ -400,10 +507,12 @@ struct T6Key {
     return isB < o.isB;
   }
 };
-size_t t6_words(const T6Key& key) {
+size_t t6_words(const T6Key& key, int form) {
   const int tr = key.isB ? T6_NC : T6_M;
   const int nks = std::max(1, (key.k + 7) / 8);
-  return (size_t)((key.rows + tr - 1) / tr) * nks * (key.isB ? T6_B_WORDS : T6_A_WORDS);
+  const size_t chunk = form == 1 ? (key.isB ? T6Form<1>::B_WORDS : T6Form<1>::A_WORDS)
+                                 : (key.isB ? T6_B_WORDS : T6_A_WORDS);
+  return (size_t)((key.rows + tr - 1) / tr) * nks * chunk;
 }
 constexpr size_t T6_PLANE_BUDGET = (size_t)4 << 30;  // bytes of planes per launch
 }  // namespace
@@ -411,6 +520,7 @@ constexpr size_t T6_PLANE_BUDGET = (size_t)4 << 30;  // bytes of planes per laun
 // Converts the distinct operands of groups [g0, g1) and launches their tiles.
 static void t6_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const std::vector<GemmGroup>& gs, size_t g0,
                       size_t g1) {
+  const int form = ctx->gemmForm;
   std::map<T6Key, size_t> where;
   size_t words = 0;
   std::vector<GemmProblem> ps;
@@ -424,7 +534,7 @@ static void t6_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
       for (const T6Key& key : {T6Key{p.A, p.lda, p.opA, p.m, p.k, 0}, T6Key{p.B, p.ldb, p.opB, p.n, p.k, 1}})
         if (!where.count(key)) {
           where[key] = words;
-          words += t6_words(key);
+          words += t6_words(key, form);
         }
       ps.push_back(p);
     }
@@ -442,9 +552,9 @@ static void t6_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
     const T6Key& key = kv.first;
     if (key.k <= 0) continue;
     const int nks = (key.k + 7) / 8, tr = key.isB ? T6_NC : T6_M;
-    ops.push_back({key.src, base + kv.second, key.rows, key.k, key.ld, key.op, key.isB, nks});
+    ops.push_back({key.src, base + kv.second, key.rows, key.k, key.ld, key.op, key.isB, nks, form});
     start.push_back(total);
-    total += (long)((key.rows + tr - 1) / tr) * tr * (nks * 8);
+    total += (long)((key.rows + tr - 1) / tr) * tr * (nks * 2);  // rows x quads of 4 complex k
   }
   for (GemmProblem& p : ps) {
     p.pa = base + where[T6Key{p.A, p.lda, p.opA, p.m, p.k, 0}];
@@ -462,6 +572,7 @@ static void t6_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
   a.ngroups = (int)groups.size();
   a.probs = nullptr;
   a.groups = nullptr;
+  a.raster = ctx->gemmRaster;
   tc_wait_args(ctx, a);
   DevBuf dp, dg;
   const bool inl = groups.size() <= (size_t)GEMM_INLINE && ps.size() <= (size_t)GEMM_INLINE;
@@ -474,12 +585,20 @@ static void t6_launch(aifmm_ctx* ctx, const std::vector<GemmProblem>& all, const
     a.probs = dp.as<GemmProblem>();
     a.groups = dg.as<GemmGroup>();
   }
-  const size_t smem = sizeof(T6Smem) + 1024;
-  smem_attr_once((const void*)zgemm_tc6_kernel<true>, ctx->device, (int)smem);
-  smem_attr_once((const void*)zgemm_tc6_kernel<false>, ctx->device, (int)smem);
   const unsigned grid = (unsigned)std::min<long>(tiles, ctx->numSMs > 0 ? ctx->numSMs : 148);
-  if (inl) zgemm_tc6_kernel<true><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
-  else zgemm_tc6_kernel<false><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
+  if (form == 1) {
+    const size_t smem = sizeof(T6Smem<1>) + 1024;
+    smem_attr_once((const void*)zgemm_tc6_kernel<1, true>, ctx->device, (int)smem);
+    smem_attr_once((const void*)zgemm_tc6_kernel<1, false>, ctx->device, (int)smem);
+    if (inl) zgemm_tc6_kernel<1, true><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
+    else zgemm_tc6_kernel<1, false><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
+  } else {
+    const size_t smem = sizeof(T6Smem<0>) + 1024;
+    smem_attr_once((const void*)zgemm_tc6_kernel<0, true>, ctx->device, (int)smem);
+    smem_attr_once((const void*)zgemm_tc6_kernel<0, false>, ctx->device, (int)smem);
+    if (inl) zgemm_tc6_kernel<0, true><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
+    else zgemm_tc6_kernel<0, false><<<grid, T6_THREADS, smem, ctx->stream>>>(a, (int)tiles);
+  }
   AIFMM_LAUNCHED();
 }
 
@@ -499,7 +618,7 @@ void zgemm_tc6(aifmm_ctx* ctx, const std::vector<GemmProblem>& ps, const std::ve
             for (const T6Key& f : fresh) dup = dup || !(f < key || key < f);
             if (!dup) {
               fresh.push_back(key);
-              add += 4 * t6_words(key);
+              add += 4 * t6_words(key, ctx->gemmForm);
             }
           }
       }

@@ -33,6 +33,20 @@ class Context:
         _lib.check(_lib.lib().aifmm_ctx_stream(self.h, C.byref(s)))
         return s.value or 0
 
+    def set_gemm_tiling(self, form: int = 0, raster: int = 0) -> None:
+        """Operand form (0 packed real, 1 split planes) and tile order (0
+        row-major, 1 column-major) of GEMM precision 4 on this context."""
+        _lib.check(_lib.lib().aifmm_ctx_set_gemm_tiling(self.h, int(form), int(raster)))
+
+    def tune_report(self) -> list[str]:
+        """The GEMM autotuner's trials on this context, one line per launch
+        class (GEMM precision 5)."""
+        n = C.c_int()
+        _lib.check(_lib.lib().aifmm_ctx_tune_report(self.h, None, 0, C.byref(n)))
+        buf = C.create_string_buffer(n.value + 1)
+        _lib.check(_lib.lib().aifmm_ctx_tune_report(self.h, buf, n.value + 1, C.byref(n)))
+        return [ln for ln in buf.value.decode().splitlines() if ln]
+
     def close(self):
         if getattr(self, "h", None):
             _lib.lib().aifmm_ctx_destroy(self.h)

@@ -92,6 +92,9 @@ def main():
         X = S.solve(B)
     t_sol = time.perf_counter() - t0
     info = S.info()
+    if a.precision == 5:
+        for line in K.ctx.tune_report():
+            print("# autotuner:", line)
     if a.profile_ops:
         from .solver import profile_ops, profile_ops_read
         S.rewind()

@@ -110,10 +110,12 @@ def test_lu_solve(nrhs):
 @pytest.mark.parametrize("precision,bound", [(0, 1e-13), (1, 2e-6), (2, 2e-6), (3, 2e-6), (4, 2e-6)])
 @pytest.mark.parametrize("m,n,k,opA,opB", [
     (64, 64, 16, 0, 0), (1, 1, 1, 0, 0), (65, 33, 17, 1, 0), (200, 130, 451, 0, 1), (37, 300, 5, 1, 1),
-    (10, 10, 0, 0, 0), (300, 260, 1000, 0, 0), (129, 257, 8, 1, 1),
+    (10, 10, 0, 0, 0), (300, 260, 1000, 0, 0), (129, 257, 8, 1, 1), (100, 60, 2000, 1, 0),
 ])
 def test_zgemm_precisions(precision, bound, m, n, k, opA, opB):
-    """Grouped GEMM in FP64 and in split TF32 (FP32-level accuracy) against numpy."""
+    """Grouped GEMM in FP64 and in split TF32 (FP32-level accuracy) against numpy.
+    Launches of a few output tiles over long depths (200 x 130 x 451, 100 x 60
+    x 2000) take the FP64 split-K path."""
     rng = np.random.default_rng(m * 7 + n * 3 + k)
     A = rng.standard_normal((k, m) if opA else (m, k)) + 1j * rng.standard_normal((k, m) if opA else (m, k))
     B = rng.standard_normal((n, k) if opB else (k, n)) + 1j * rng.standard_normal((n, k) if opB else (k, n))
@@ -163,4 +165,25 @@ def test_tensor_core_wait_timeout_is_an_error(precision):
     assert n1.value - n0.value == (2 if precision == 4 else 2 * 2)
     C = lowrank.zgemm(A, B, precision=precision, ctx=ctx)  # the same context afterwards
     assert np.linalg.norm(C - A @ B) <= 2e-6 * np.linalg.norm(A) * np.linalg.norm(B)
+    ctx.close()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("form,raster", [(0, 1), (1, 0), (1, 1)])
+@pytest.mark.parametrize("m,n,k,opA,opB", [(200, 130, 451, 0, 1), (300, 260, 1000, 0, 0), (129, 257, 8, 1, 1),
+                                           (65, 33, 17, 1, 0)])
+def test_persistent_gemm_forms(form, raster, m, n, k, opA, opB):
+    """The persistent tensor-core GEMM in both operand forms and both tile
+    orders: FP32-class accuracy, not an FP64 product, no wait ran out."""
+    from rcs_b200.kernel import Context
+    ctx = Context(0)
+    ctx.set_gemm_tiling(form, raster)
+    rng = np.random.default_rng(m + n + k)
+    A = rng.standard_normal((k, m) if opA else (m, k)) + 1j * rng.standard_normal((k, m) if opA else (m, k))
+    B = rng.standard_normal((n, k) if opB else (k, n)) + 1j * rng.standard_normal((n, k) if opB else (k, n))
+    C0 = rng.standard_normal((m, n)) + 1j * rng.standard_normal((m, n))
+    C = lowrank.zgemm(A, B, opA, opB, 0.5 - 2j, 1.0 + 0.25j, C0, precision=4, ctx=ctx)
+    ref = (0.5 - 2j) * ((A.conj().T if opA else A) @ (B.conj().T if opB else B)) + (1.0 + 0.25j) * C0
+    scale = abs(0.5 - 2j) * np.linalg.norm(A) * np.linalg.norm(B) + abs(1.0 + 0.25j) * np.linalg.norm(C0)
+    assert 1e-12 * scale <= np.linalg.norm(C - ref) <= 2e-6 * scale
     ctx.close()
