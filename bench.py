@@ -394,6 +394,7 @@ def run_batch(args, rank, world, local):
                   precision=cfg["precision"], drop_pow=cfg["drop_pow"])
         S.checkpoint()
         A = H2Operator(K, leaf_size=cfg["leaf"], tol_pow=cfg["op_tol"])
+        ctx.trim()  # the assembly's temporaries go back to the device for the next bodies
         bodies.append(dict(ctx=ctx, K=K, S=S, A=A, B=B, axes=axes))
     t_setup = time.perf_counter() - t0
     Ss, As, Bs = [b["S"] for b in bodies], [b["A"] for b in bodies], [b["B"] for b in bodies]
@@ -425,6 +426,7 @@ def run_batch(args, rank, world, local):
         torch.cuda.synchronize()
     launches = launch_count() - l0
     t_step = max_over_ranks(e0.elapsed_time(e1) / 1e3 / args.steps, world)
+    mem = [b["ctx"].memory() for b in bodies]
     res = [sampled_residual(b["K"], x, b["B"], nrows=256) for b, x in zip(bodies, out["xs"])]
     # the plain FP64 path, one body after another (one timed pass)
     plain = None
@@ -456,6 +458,8 @@ def run_batch(args, rank, world, local):
             "residual_max": float(max(res)), "residual_per_body": [float(r) for r in res],
             "gmres_iterations": [r["iterations"] for r in out["recs"]],
             "plain_fp64": plain, "setup_s": t_setup, "gpu_launches": int(launches), "clocks": clk.summary(),
+            "device_gb_after_step": {"live": sum(m["live"] for m in mem) / 1e9,
+                                     "reserved": sum(m["reserved"] for m in mem) / 1e9},
             "e2e": {"value": t_step, "unit": "s", "h2d_bytes_per_step": int(16 * sum(Ns) * cfg["nrhs"]),
                     "d2h_bytes_per_step": int(16 * sum(Ns) * cfg["nrhs"]),
                     "note": "the batch entry points take host right-hand sides and return host solutions"},

@@ -61,6 +61,16 @@ int aifmm_ctx_tune_report(aifmm_ctx* ctx, char* buf, int cap, int* len);
  * tile order (0 row-major: the default, 1 column-major) of GEMM precision 4
  * on this context, the autotuner's knobs (no counterpart in the reference). */
 int aifmm_ctx_set_gemm_tiling(aifmm_ctx* ctx, int form, int raster);
+/* Device memory of the context: *live = bytes of the buffers its objects
+ * hold, *reserved = bytes its memory pool holds from the device (live
+ * buffers, the arena's chunks and freed blocks kept for reuse).  Either
+ * pointer may be NULL. */
+int aifmm_ctx_memory(aifmm_ctx* ctx, size_t* live, size_t* reserved);
+/* Waits for the context's stream, then returns to the device the arena
+ * chunks that hold no buffer and the blocks its pool keeps for reuse, so
+ * that other contexts on the device can use them (a batch of bodies trims
+ * each body's context after its factorization and after its solve). */
+int aifmm_ctx_trim(aifmm_ctx* ctx);
 
 /* ---- matrix-entry kernels ------------------------------------------------ */
 /* EFIE kernel over a flat-triangle mesh: replaces
@@ -235,6 +245,9 @@ typedef struct {
    * launches (reruns included), number of launches */
   double t_aca, aca_ws_bytes;
   long n_aca_launches;
+  /* solves replayed from a captured CUDA graph of the solve sweep, and
+   * graphs captured (one per factorization and right-hand-side count) */
+  long n_solve_graph, n_solve_capture;
 } aifmm_solver_info;
 
 /* AIFMM<K>::AIFMM(inputsToSolverClass, K*) (src/AIFMM.cpp:7-93): builds the
@@ -260,6 +273,12 @@ int aifmm_solver_factorize(aifmm_solver* s);
 int aifmm_solver_solve(aifmm_solver* s, const double* rhs, int nrhs, double* x);
 /* Same with device pointers (complex128, n x nrhs, ld = n). */
 int aifmm_solver_solve_device(aifmm_solver* s, const void* rhs_device, int nrhs, void* x_device);
+/* on = 1 (the default): the first solve for a right-hand-side count after a
+ * factorization captures the whole solve sweep as a CUDA graph, and solves
+ * replay it (same kernels, same results, one launch from the host); on = 0:
+ * every solve issues its kernels one by one.  The per-launch profilers of
+ * this library turn replays off while they run. */
+int aifmm_solver_set_graph_solve(aifmm_solver* s, int on);
 /* Tree statistics and phase timings (getAvgLeafSize, getAvgMultipoles,
  * findMemory*, T:490-552 and T:4511-4571 of the tree header). */
 int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info);

@@ -34,6 +34,8 @@ SIGNATURES = {
     "aifmm_ctx_stream": (_i, [_p, _pp]),
     "aifmm_ctx_tune_report": (_i, [_p, C.c_char_p, _i, C.POINTER(_i)]),
     "aifmm_ctx_set_gemm_tiling": (_i, [_p, _i, _i]),
+    "aifmm_ctx_memory": (_i, [_p, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t)]),
+    "aifmm_ctx_trim": (_i, [_p]),
     "aifmm_kernel_create_efie": (_i, [_p, _dp, _i, _ip, _i, _d, _pp]),
     "aifmm_kernel_create_es": (_i, [_p, _dp, _i, _ip, _p, _i, _pp]),
     "aifmm_kernel_destroy": (_i, [_p]),
@@ -52,6 +54,7 @@ SIGNATURES = {
     "aifmm_solver_tree_order": (_i, [_p, _ip]),
     "aifmm_solver_factorize": (_i, [_p]),
     "aifmm_solver_solve": (_i, [_p, _dp, _i, _dp]),
+    "aifmm_solver_set_graph_solve": (_i, [_p, _i]),
     "aifmm_solver_solve_device": (_i, [_p, _p, _i, _p]),
     "aifmm_solver_get_info": (_i, [_p, _p]),
     "aifmm_solver_destroy": (_i, [_p]),
@@ -115,7 +118,7 @@ class SolverInfo(C.Structure):
                 ("t_compress", C.c_double), ("t_elim_x", C.c_double), ("t_elim_z", C.c_double),
                 ("t_nonleaf", C.c_double), ("t_lu", C.c_double), ("t_msolve", C.c_double),
                 ("t_schur", C.c_double), ("t_aca", C.c_double), ("aca_ws_bytes", C.c_double),
-                ("n_aca_launches", C.c_long)]
+                ("n_aca_launches", C.c_long), ("n_solve_graph", C.c_long), ("n_solve_capture", C.c_long)]
 
 class GmresInfo(C.Structure):
     _fields_ = [("iterations", C.c_int), ("cycles", C.c_int), ("relres", C.c_double), ("t_precond", C.c_double),

@@ -4,7 +4,9 @@
 // The factorization allocates and frees hundreds of thousands of blocks of
 // every size; each stream-ordered pool call for a large block costs tens of
 // microseconds to milliseconds of host time.  The arena carves such blocks
-// out of chunks it keeps (1 GB, or one request's size when larger): a free
+// out of chunks it keeps -- 64 MB at first, each new chunk as large as all
+// earlier ones together up to 1 GB (so a small body's context, one of a
+// batch of dozens, holds little), or one request's size when larger: a free
 // block is found by size in a multimap, split, and merged with its free
 // neighbours of the same chunk when released.  Every use of context memory
 // is ordered on the context's one stream, so a released range can be handed
@@ -25,7 +27,8 @@ namespace aifmm {
 class Arena {
  public:
   static constexpr size_t kAlign = 512;
-  static constexpr size_t kChunk = (size_t)1 << 30;
+  static constexpr size_t kChunk = (size_t)1 << 30;       // largest growth step
+  static constexpr size_t kFirstChunk = (size_t)64 << 20;  // first growth step
   static constexpr size_t kMinSize = (size_t)256 << 10;
 
   // grow(bytes) returns the base address of a new chunk of `bytes` bytes, or 0.
@@ -38,10 +41,13 @@ class Arena {
     const size_t need = round(n == 0 ? 1 : n);
     auto it = bySize_.lower_bound(need);
     if (it == bySize_.end()) {
-      const size_t bytes = need > kChunk ? need : kChunk;
+      // geometric growth: as much as the chunks held so far, at least the first step, at most kChunk
+      const size_t step = bytesHeld_ < kFirstChunk ? kFirstChunk : (bytesHeld_ > kChunk ? kChunk : bytesHeld_);
+      const size_t bytes = need > step ? need : step;
       const uint64_t base = grow_(bytes);
       if (base == 0) return 0;
       chunks_[base] = bytes;
+      bytesHeld_ += bytes;
       insertFree(base, bytes);
       it = bySize_.lower_bound(need);
     }
@@ -94,6 +100,7 @@ class Arena {
       if (f != byAddr_.end() && f->second == c->second) {
         eraseFree(f->first, f->second);
         out.push_back(*c);
+        bytesHeld_ -= c->second;
         c = chunks_.erase(c);
       } else {
         ++c;
@@ -132,6 +139,7 @@ class Arena {
   std::multimap<size_t, uint64_t> bySize_;
   std::map<uint64_t, size_t> used_;     // handed-out ranges
   size_t bytesUsed_ = 0;
+  size_t bytesHeld_ = 0;  // bytes of all chunks held
 };
 
 }  // namespace aifmm

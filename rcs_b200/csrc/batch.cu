@@ -85,8 +85,9 @@ int aifmm_batch_factorize(aifmm_solver* const* solvers, int n, int threads, doub
   std::string msg;
   const int rc = run_pool(n, threads, [&](int i) {
     Solver& S = *solvers[i]->s;
+    AIFMM_CUDA(cudaSetDevice(S.ctx->device));
     S.factorize();
-    AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
+    ctx_trim(S.ctx);  // the elimination's temporaries go back to the device for the other bodies
   }, msg);
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (rc != AIFMM_OK) throw Error(rc, msg);
@@ -115,6 +116,8 @@ int aifmm_batch_solve_gmres(aifmm_solver* const* solvers, aifmm_operator* const*
     AIFMM_CUDA(cudaMemcpyAsync(x[i], xd.p, bytes, cudaMemcpyDeviceToHost, S.ctx->stream));
     AIFMM_CUDA(cudaStreamSynchronize(S.ctx->stream));
     if (info) fill_gmres_info(r, &info[i]);
+    S.dropPlan();  // the captured sweep's intermediates
+    ctx_trim(S.ctx);
   }, msg);
   if (seconds) *seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
   if (rc != AIFMM_OK) throw Error(rc, msg);

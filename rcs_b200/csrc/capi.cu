@@ -56,6 +56,7 @@ void ctx_release(aifmm_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
   }
   if (c->pool) cudaMemPoolDestroy(c->pool);
+  if (c->sideStream) cudaStreamDestroy(c->sideStream);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c;
 }
@@ -67,10 +68,19 @@ static void arena_trim(aifmm_ctx* c) {
   for (auto& ch : c->arena->takeFreeChunks()) cudaFreeAsync((void*)ch.first, c->stream);
 }
 
+void ctx_trim(aifmm_ctx* c) {
+  AIFMM_REQUIRE(!c->capture, AIFMM_ESTATE, "trim during a graph capture");
+  AIFMM_CUDA(cudaStreamSynchronize(c->stream));
+  arena_trim(c);
+  AIFMM_CUDA(cudaStreamSynchronize(c->stream));
+  AIFMM_CUDA(cudaMemPoolTrimTo(c->pool, 0));
+}
+
 void DevBuf::alloc(aifmm_ctx* c, size_t n) {
   release();
   ctx = c;
   bytes = n;
+  hold = c->capture;
   if (c->arena && n >= Arena::kMinSize) {
     std::lock_guard<std::mutex> l(c->arenaMu);
     const uint64_t a = c->arena->alloc(n);
@@ -82,14 +92,17 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
     }
   }
   const double t0 = opprof::enabled() ? opprof::now() : 0.0;
-  cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, c->stream);
+  // during a capture the allocation is made outside it, on the side stream
+  cudaStream_t s = c->capture ? c->sideStream : c->stream;
+  cudaError_t e = cudaMallocFromPoolAsync(&p, n, c->pool, s);
+  if (e == cudaSuccess && c->capture) e = cudaStreamSynchronize(s);
   if (opprof::enabled()) {
     const double dt = opprof::now() - t0;
     opprof::add("pool_alloc", dt);
     opprof::add(n < ((size_t)1 << 20) ? "pool_alloc_lt1MB" : n < ((size_t)64 << 20) ? "pool_alloc_lt64MB" : "pool_alloc_ge64MB",
                 dt);
   }
-  if (e == cudaErrorMemoryAllocation) {
+  if (e == cudaErrorMemoryAllocation && !c->capture) {  // (a capturing stream cannot be drained)
     // the pool and the arena keep freed blocks; return them to the device and retry once
     cudaGetLastError();
     arena_trim(c);
@@ -106,6 +119,11 @@ void DevBuf::alloc(aifmm_ctx* c, size_t n) {
 }
 void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
   if (n == 0) return;
+  if (c->capture) {  // copied now, outside the capture: dst is a buffer the graph holds
+    AIFMM_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, c->sideStream));
+    AIFMM_CUDA(cudaStreamSynchronize(c->sideStream));
+    return;
+  }
   if (!c->ring || n > aifmm_ctx::kRingBytes / 4) {
     AIFMM_CUDA(cudaMemcpyAsync(dst, src, n, cudaMemcpyHostToDevice, c->stream));
     return;
@@ -132,6 +150,28 @@ void upload_bytes(aifmm_ctx* c, void* dst, const void* src, size_t n) {
 }
 
 void DevBuf::release() {
+  if (p && ctx) {
+    // A buffer allocated during a capture stays with that graph while the
+    // graph lives.  Any other buffer released while a capture is in progress
+    // may be read by a node captured before the release, so the capture in
+    // progress keeps it (and a free on the capturing stream would be a graph
+    // node of memory the graph does not own).
+    std::shared_ptr<CaptureHold> own = std::move(hold);
+    const std::shared_ptr<CaptureHold> cur = ctx->capture;
+    const std::shared_ptr<CaptureHold>* holds[2] = {&own, &cur};
+    for (const std::shared_ptr<CaptureHold>* h : holds) {
+      if (!*h) continue;
+      std::lock_guard<std::mutex> l((*h)->mu);
+      if ((*h)->alive) {
+        (*h)->held.push_back({p, bytes, fromArena});
+        p = nullptr;
+        bytes = 0;
+        fromArena = false;
+        return;
+      }
+    }
+  }
+  hold.reset();
   if (p && ctx && fromArena) {
     {
       std::lock_guard<std::mutex> l(ctx->arenaMu);
@@ -151,6 +191,22 @@ void DevBuf::release() {
   }
   p = nullptr;
   bytes = 0;
+}
+
+void CaptureHold::releaseAll() {
+  std::vector<Rec> recs;
+  {
+    std::lock_guard<std::mutex> l(mu);
+    alive = false;
+    recs.swap(held);
+  }
+  for (const Rec& r : recs) {
+    DevBuf b;  // no hold: released at once
+    b.ctx = ctx;
+    b.p = r.p;
+    b.bytes = r.bytes;
+    b.fromArena = r.fromArena;
+  }
 }
 
 }  // namespace aifmm
@@ -227,7 +283,9 @@ int aifmm_ctx_create(int device, aifmm_ctx** out) {
     aifmm_ctx* cp = c.get();
     c->arena.reset(new Arena([cp](size_t bytes) -> uint64_t {
       void* q = nullptr;
-      if (cudaMallocFromPoolAsync(&q, bytes, cp->pool, cp->stream) != cudaSuccess) {
+      cudaStream_t s = cp->capture ? cp->sideStream : cp->stream;  // outside a capture in progress
+      if (cudaMallocFromPoolAsync(&q, bytes, cp->pool, s) != cudaSuccess ||
+          (cp->capture && cudaStreamSynchronize(s) != cudaSuccess)) {
         cudaGetLastError();
         return 0;
       }
@@ -269,6 +327,26 @@ int aifmm_ctx_set_gemm_tiling(aifmm_ctx* ctx, int form, int raster) {
                 "form and raster must be 0 or 1");
   ctx->gemmForm = form;
   ctx->gemmRaster = raster;
+  API_END
+}
+
+int aifmm_ctx_memory(aifmm_ctx* ctx, size_t* live, size_t* reserved) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx, AIFMM_EINVAL, "NULL context");
+  if (live) *live = ctx->bytes_live;
+  if (reserved) {
+    unsigned long long r = 0;  // the attribute is a 64-bit unsigned value
+    AIFMM_CUDA(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrReservedMemCurrent, &r));
+    *reserved = (size_t)r;
+  }
+  API_END
+}
+
+int aifmm_ctx_trim(aifmm_ctx* ctx) {
+  API_BEGIN
+  AIFMM_REQUIRE(ctx, AIFMM_EINVAL, "NULL context");
+  AIFMM_CUDA(cudaSetDevice(ctx->device));
+  ctx_trim(ctx);
   API_END
 }
 

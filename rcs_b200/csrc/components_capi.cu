@@ -112,6 +112,7 @@ static void rrqr_host(aifmm_ctx* ctx, const double* A, int m, int n, int partiti
   } h;
   AIFMM_CUDA(cudaMemcpyAsync(&h, out.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
   AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  AIFMM_REQUIRE(h.r != -2, AIFMM_ETIMEOUT, "RRQR: a bounded grid-barrier wait ran out");
   *rank = h.r;
   *max_pivot = h.mp;
   if (h.r > 0)

@@ -10,6 +10,10 @@
 #include "arena.cuh"
 #include "assemble.cuh"
 
+namespace aifmm {
+struct CaptureHold;
+}
+
 // Objects created on a context (kernels, solvers) hold a reference; the
 // context's stream and memory pool are released when aifmm_ctx_destroy has
 // been called and the last such object is gone, so destruction order does
@@ -58,14 +62,42 @@ struct aifmm_ctx {
   // come from `pool`.  Created with the context.
   std::mutex arenaMu;
   std::unique_ptr<aifmm::Arena> arena;
+  // While a CUDA graph is being captured on `stream` (the solver's solve
+  // plans), `capture` is set: device allocations and host uploads then go
+  // through `sideStream`, outside the capture, and every buffer allocated
+  // during the capture stays reserved for the graph until the graph is
+  // destroyed (CaptureHold).
+  std::shared_ptr<aifmm::CaptureHold> capture;
+  cudaStream_t sideStream = nullptr;
 };
 
 namespace aifmm {
 void ctx_retain(aifmm_ctx* c);
 void ctx_release(aifmm_ctx* c);
+// Drains the stream and returns unused arena chunks and pooled blocks to the device.
+void ctx_trim(aifmm_ctx* c);
 }  // namespace aifmm
 
 namespace aifmm {
+
+// Device memory that a captured CUDA graph reads or writes.  A replay of the
+// graph touches the addresses it was captured with, so none of them may go
+// back to the pool or the arena while the graph exists: a buffer allocated
+// during the capture carries the hold, and its release only records it here.
+// releaseAll(), called once the graph is destroyed, returns what was recorded;
+// buffers released after that go back at once.
+struct CaptureHold {
+  struct Rec {
+    void* p;
+    size_t bytes;
+    bool fromArena;
+  };
+  aifmm_ctx* ctx = nullptr;
+  std::mutex mu;
+  bool alive = true;
+  std::vector<Rec> held;
+  void releaseAll();
+};
 
 // Device buffer allocated from the context's stream-ordered pool.
 struct DevBuf {
@@ -73,11 +105,12 @@ struct DevBuf {
   void* p = nullptr;
   size_t bytes = 0;
   bool fromArena = false;  // p came from the context's arena, not the pool
+  std::shared_ptr<CaptureHold> hold;  // allocated while a graph was captured
   DevBuf() {}
   DevBuf(aifmm_ctx* c, size_t n) { alloc(c, n); }
   DevBuf(const DevBuf&) = delete;
   DevBuf& operator=(const DevBuf&) = delete;
-  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), bytes(o.bytes), fromArena(o.fromArena) {
+  DevBuf(DevBuf&& o) noexcept : ctx(o.ctx), p(o.p), bytes(o.bytes), fromArena(o.fromArena), hold(std::move(o.hold)) {
     o.p = nullptr;
     o.bytes = 0;
     o.fromArena = false;
@@ -85,7 +118,7 @@ struct DevBuf {
   DevBuf& operator=(DevBuf&& o) noexcept {
     if (this != &o) {
       release();
-      ctx = o.ctx; p = o.p; bytes = o.bytes; fromArena = o.fromArena;
+      ctx = o.ctx; p = o.p; bytes = o.bytes; fromArena = o.fromArena; hold = std::move(o.hold);
       o.p = nullptr; o.bytes = 0; o.fromArena = false;
     }
     return *this;

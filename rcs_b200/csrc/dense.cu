@@ -143,18 +143,28 @@ __global__ void __launch_bounds__(256, 2) zgemm_grouped_kernel(const __grid_cons
   const GemmProblem& P = probs[g.head];
   const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
   const bool beta0 = (P.beta.x == 0.0 && P.beta.y == 0.0);
+  // each row's 4 C entries are loaded together before its stores, so an
+  // accumulating tile waits for memory 4 times instead of 16 (a whole
+  // micro-tile at once would spill: the kernel is at its register cap)
 #pragma unroll
   for (int i = 0; i < 4; ++i) {
     const int r = row0 + tx + 16 * i;
     if (r >= P.m) continue;
+    zd cv[4];
+    if (!beta0) {
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const int c = col0 + ty + 16 * j;
+        if (c < P.n) cv[j] = __ldcg(P.C + (size_t)c * P.ldc + r);
+      }
+    }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
       const int c = col0 + ty + 16 * j;
       if (c >= P.n) continue;
-      zd* cp = P.C + (size_t)c * P.ldc + r;
       zd v = zmul(P.alpha, acc[i][j]);
-      if (!beta0) v = zadd(v, zmul(P.beta, *cp));
-      *cp = v;
+      if (!beta0) v = zadd(v, zmul(P.beta, cv[j]));
+      P.C[(size_t)c * P.ldc + r] = v;
     }
   }
 }
@@ -929,7 +939,10 @@ __global__ void __launch_bounds__(1024) zgetrf_panel_kernel(zd* A, int n, int ld
 }
 
 // X <- T^{-1} X for a triangular nb x nb block T (unit lower or non-unit
-// upper) and X = nb rows x ncols columns; one thread per column.
+// upper) and X = nb rows x ncols columns; one thread per column, launched
+// kTrsmThreads to a CTA so that a box's few hundred columns spread over as
+// many SMs.
+constexpr int kTrsmThreads = 32;
 template <bool LOWER_UNIT>
 __global__ void ztrsm_block_kernel(const zd* __restrict__ T, int ldt, int nb, zd* X, int ldx, int ncols) {
   __shared__ zd Ts[LU_NB * LU_NB];
@@ -978,6 +991,57 @@ __global__ void zlaswp_kernel(zd* B, int ldb, int nrhs, const int* __restrict__ 
   }
 }
 
+// The row interchanges of an LU solve as one gather per column: every CTA
+// first composes the n interchanges into the permutation src (row i of the
+// result is row src[i] of the input: the swaps replayed in order on an index
+// array in shared memory), then each warp copies its column through shared
+// memory.  The same result as applying the swaps one by one, without one
+// thread walking n dependent swaps per column.
+__global__ void zlaswp_perm_kernel(zd* B, int ldb, int nrhs, const int* __restrict__ piv, int n) {
+  extern __shared__ __align__(16) unsigned char laswp_sm[];
+  int* src = reinterpret_cast<int*>(laswp_sm);
+  int* pv = src + n;
+  zd* buf = reinterpret_cast<zd*>(laswp_sm + (((size_t)2 * n * sizeof(int) + 15) & ~(size_t)15));
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    src[i] = i;
+    pv[i] = piv[i];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int k = 0; k < n; ++k) {
+      const int p = pv[k];
+      if (p != k) {
+        const int t = src[k];
+        src[k] = src[p];
+        src[p] = t;
+      }
+    }
+  __syncthreads();
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  const int c = blockIdx.x * nw + w;
+  if (c >= nrhs) return;
+  zd* b = B + (size_t)c * ldb;
+  zd* t = buf + (size_t)w * n;
+  for (int i = lane; i < n; i += 32) t[i] = b[src[i]];
+  __syncwarp();
+  for (int i = lane; i < n; i += 32) b[i] = t[i];
+}
+
+static void zlaswp(aifmm_ctx* ctx, zd* B, int ldb, int nrhs, const int* piv, int n) {
+  constexpr size_t kSmemMax = 200 * 1024;
+  const size_t idx = ((size_t)2 * n * sizeof(int) + 15) & ~(size_t)15;
+  const size_t perWarp = sizeof(zd) * (size_t)n;
+  const int warps = (int)std::min<size_t>(8, idx + perWarp <= kSmemMax ? (kSmemMax - idx) / perWarp : 0);
+  if (warps == 0) {  // a column does not fit in shared memory: the swaps one by one
+    zlaswp_kernel<<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(B, ldb, nrhs, piv, n);
+    AIFMM_LAUNCHED();
+    return;
+  }
+  smem_attr_once((const void*)zlaswp_perm_kernel, ctx->device, (int)kSmemMax);
+  zlaswp_perm_kernel<<<ceil_div(nrhs, warps), 32 * warps, idx + perWarp * warps, ctx->stream>>>(B, ldb, nrhs, piv, n);
+  AIFMM_LAUNCHED();
+}
+
 void zgetrf(aifmm_ctx* ctx, zd* A, int n, int lda, int* piv, int* info) {
   if (n <= 0) return;
   AIFMM_CUDA(cudaMemsetAsync(info, 0, sizeof(int), ctx->stream));
@@ -988,7 +1052,7 @@ void zgetrf(aifmm_ctx* ctx, zd* A, int n, int lda, int* piv, int* info) {
     const int rest = n - j0 - nb;
     if (rest <= 0) continue;
     // U12 = L11^{-1} A12
-    ztrsm_block_kernel<true><<<ceil_div(rest, 128), 128, 0, ctx->stream>>>(A + (size_t)j0 * lda + j0, lda, nb,
+    ztrsm_block_kernel<true><<<ceil_div(rest, kTrsmThreads), kTrsmThreads, 0, ctx->stream>>>(A + (size_t)j0 * lda + j0, lda, nb,
                                                                            A + (size_t)(j0 + nb) * lda + j0, lda,
                                                                            rest);
     AIFMM_LAUNCHED();
@@ -1085,12 +1149,11 @@ void zgetrs(aifmm_ctx* ctx, const zd* LU, int n, int lda, const int* piv, zd* B,
     AIFMM_LAUNCHED();
     return;
   }
-  zlaswp_kernel<<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(B, ldb, nrhs, piv, n);
-  AIFMM_LAUNCHED();
+  zlaswp(ctx, B, ldb, nrhs, piv, n);
   // forward: unit lower
   for (int i0 = 0; i0 < n; i0 += LU_NB) {
     const int nb = std::min(LU_NB, n - i0);
-    ztrsm_block_kernel<true><<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
+    ztrsm_block_kernel<true><<<ceil_div(nrhs, kTrsmThreads), kTrsmThreads, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
                                                                            B + i0, ldb, nrhs);
     AIFMM_LAUNCHED();
     const int rest = n - i0 - nb;
@@ -1104,7 +1167,7 @@ void zgetrs(aifmm_ctx* ctx, const zd* LU, int n, int lda, const int* piv, zd* B,
   const int last = ((n - 1) / LU_NB) * LU_NB;
   for (int i0 = last; i0 >= 0; i0 -= LU_NB) {
     const int nb = std::min(LU_NB, n - i0);
-    ztrsm_block_kernel<false><<<ceil_div(nrhs, 128), 128, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
+    ztrsm_block_kernel<false><<<ceil_div(nrhs, kTrsmThreads), kTrsmThreads, 0, ctx->stream>>>(LU + (size_t)i0 * lda + i0, lda, nb,
                                                                             B + i0, ldb, nrhs);
     AIFMM_LAUNCHED();
     if (i0 > 0) {

@@ -541,8 +541,7 @@ __device__ inline void rrqr_p2_bounds(const RRQRProblem& P, int& first, int& ste
   if (P.p2cap >= 0) steps = min(steps, first + P.p2cap);
 }
 
-__global__ void rrqr_p2_init_kernel(const RRQRProblem* __restrict__ probs) {
-  const RRQRProblem P = probs[blockIdx.x];
+__device__ void rrqr_p2_init_body(const RRQRProblem& P) {
   for (int q = P.istate[1] + threadIdx.x; q < P.partition; q += blockDim.x) P.nsq[q] = 0.0;
   if (threadIdx.x == 0) {
     P.istate[4] = 0;
@@ -551,12 +550,10 @@ __global__ void rrqr_p2_init_kernel(const RRQRProblem* __restrict__ probs) {
     P.istate[7] = 0;
   }
 }
+__global__ void rrqr_p2_init_kernel(const RRQRProblem* __restrict__ probs) { rrqr_p2_init_body(probs[blockIdx.x]); }
 
-__global__ void __launch_bounds__(QR_NT) rrqr_p2_pivot_kernel(const RRQRProblem* __restrict__ probs, int t) {
-  __shared__ double shv[33];
-  __shared__ int shi[33];
-  __shared__ zd s_alpha;
-  const RRQRProblem P = probs[blockIdx.x];
+// one CTA of QR_NT threads
+__device__ void rrqr_p2_pivot_body(const RRQRProblem& P, int t, double* shv, int* shi, zd& s_alpha) {
   const int tid = threadIdx.x, m = P.m, n = P.n;
   if (P.istate[4]) {  // stopped earlier: nothing to apply
     if (tid == 0) P.istate[6] = -1;
@@ -642,17 +639,19 @@ __global__ void __launch_bounds__(QR_NT) rrqr_p2_pivot_kernel(const RRQRProblem*
     }
   }
 }
+__global__ void __launch_bounds__(QR_NT) rrqr_p2_pivot_kernel(const RRQRProblem* __restrict__ probs, int t) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  rrqr_p2_pivot_body(probs[blockIdx.x], t, shv, shi, s_alpha);
+}
 
 // The committed reflector of the step applied to the columns at positions
 // >= j, one warp per column, with the pivot column's sub-diagonal zeroed and
 // the downdates of the norms at positions > j.
-__global__ void rrqr_p2_apply_kernel(const RRQRProblem* __restrict__ probs) {
-  const RRQRProblem P = probs[blockIdx.y];
-  const int j = P.istate[6];
-  if (j < 0) return;
-  const int m = P.m, lane = threadIdx.x & 31;
-  const int q = j + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (q >= P.n) return;
+// column at position q (>= j) by one warp
+__device__ void rrqr_p2_apply_col(const RRQRProblem& P, int j, int q, int lane) {
+  const int m = P.m;
   const zd* h = P.H + (size_t)P.istate[7] * m;
   zd* y = P.R + (size_t)P.perm[q] * m;
   zd a = zmk(0, 0);
@@ -670,9 +669,16 @@ __global__ void rrqr_p2_apply_kernel(const RRQRProblem* __restrict__ probs) {
     P.nsq[q] = P.nsq[q] - ab * ab;
   }
 }
+__global__ void rrqr_p2_apply_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int j = P.istate[6];
+  if (j < 0) return;
+  const int q = j + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= P.n) return;
+  rrqr_p2_apply_col(P, j, q, threadIdx.x & 31);
+}
 
-__global__ void rrqr_p2_finish_kernel(const RRQRProblem* __restrict__ probs) {
-  const RRQRProblem P = probs[blockIdx.x];
+__device__ void rrqr_p2_finish_body(const RRQRProblem& P) {
   if (threadIdx.x != 0) return;
   int first, steps;
   rrqr_p2_bounds(P, first, steps);
@@ -683,13 +689,11 @@ __global__ void rrqr_p2_finish_kernel(const RRQRProblem* __restrict__ probs) {
   *P.rank = rank;
   *P.maxPivot = P.dstate[1];
 }
+__global__ void rrqr_p2_finish_kernel(const RRQRProblem* __restrict__ probs) { rrqr_p2_finish_body(probs[blockIdx.x]); }
 
 // Partition 1 on the old-basis panel (positions [0, partition)).
-__global__ void __launch_bounds__(QR_NT) rrqr_p1_kernel(const RRQRProblem* __restrict__ probs) {
-  __shared__ double shv[33];
-  __shared__ int shi[33];
-  __shared__ zd s_alpha;
-  const RRQRProblem P = probs[blockIdx.x];
+// one CTA of QR_NT threads
+__device__ void rrqr_p1_body(const RRQRProblem& P, double* shv, int* shi, zd& s_alpha) {
   const int tid = threadIdx.x, m = P.m, n = P.n;
   const int warp = tid >> 5, lane = tid & 31, nwarp = QR_NT / 32;
   for (int q = tid; q < n; q += QR_NT) P.perm[q] = q;
@@ -715,15 +719,18 @@ __global__ void __launch_bounds__(QR_NT) rrqr_p1_kernel(const RRQRProblem* __res
     P.dstate[1] = maxPivot;
   }
 }
+__global__ void __launch_bounds__(QR_NT) rrqr_p1_kernel(const RRQRProblem* __restrict__ probs) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  rrqr_p1_body(probs[blockIdx.x], shv, shi, s_alpha);
+}
 
 // The committed partition-1 reflectors applied to every fill-in column (one
 // warp per column), with the reference's norm downdates in step order.
-__global__ void rrqr_fill_kernel(const RRQRProblem* __restrict__ probs) {
-  const RRQRProblem P = probs[blockIdx.y];
+// fill-in column q by one warp
+__device__ void rrqr_fill_col(const RRQRProblem& P, int q, int lane) {
   const int m = P.m;
-  const int lane = threadIdx.x & 31;
-  const int q = P.partition + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  if (q >= P.n) return;
   const int nref = P.istate[0];
   zd* y = P.R + (size_t)q * m;
   double s = 0.0;
@@ -744,6 +751,12 @@ __global__ void rrqr_fill_kernel(const RRQRProblem* __restrict__ probs) {
     nsq = nsq - ab * ab;
   }
   if (lane == 0) P.nsq[q] = nsq;
+}
+__global__ void rrqr_fill_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int q = P.partition + blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (q >= P.n) return;
+  rrqr_fill_col(P, q, threadIdx.x & 31);
 }
 
 // Partition 2 over positions [first, n), then the rank and outputs.
@@ -777,13 +790,10 @@ __global__ void __launch_bounds__(QR_NT) rrqr_p2_kernel(const RRQRProblem* __res
 }
 
 // Q_trunc column c = H_0 ... H_{nref-1} e_c, one warp per column.
-__global__ void rrqr_q_kernel(const RRQRProblem* __restrict__ probs) {
-  const RRQRProblem P = probs[blockIdx.y];
+// Q_trunc column c (< rank) by one warp
+__device__ void rrqr_q_col(const RRQRProblem& P, int c, int lane) {
   const int m = P.m;
-  const int lane = threadIdx.x & 31;
-  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-  const int nref = P.istate[2], rank = P.istate[3];
-  if (c >= rank) return;
+  const int nref = P.istate[2];
   zd* y = P.Q + (size_t)c * m;
   for (int i = lane; i < m; i += 32) y[i] = (i == c) ? zmk(1, 0) : zmk(0, 0);
   __syncwarp();
@@ -798,6 +808,92 @@ __global__ void rrqr_q_kernel(const RRQRProblem* __restrict__ probs) {
     for (int i = lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
     __syncwarp();
   }
+}
+__global__ void rrqr_q_kernel(const RRQRProblem* __restrict__ probs) {
+  const RRQRProblem P = probs[blockIdx.y];
+  const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (c >= P.istate[3]) return;
+  rrqr_q_col(P, c, threadIdx.x & 31);
+}
+
+// ---- the split pipeline of one problem as one cooperative launch
+// The same device bodies as the per-step launches (so the same arithmetic,
+// bit for bit), separated by grid-wide barriers instead of kernel
+// boundaries: CTA 0 runs the single-CTA phases (partition 1, each step's
+// pivot and reflector, the outputs), every warp of the grid the per-column
+// phases.  A cooperative launch makes every CTA resident at once, so the
+// barriers complete; each wait is still bounded (one second) and a barrier
+// that runs out marks the problem's rank -2 (the host reports a timeout).
+__device__ __forceinline__ unsigned long long rrqr_now() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+__device__ bool rrqr_grid_sync(unsigned* bar, unsigned target, int* err) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(bar, 1u);
+    const unsigned long long t0 = rrqr_now();
+    while (*(volatile unsigned*)bar < target) {
+      if (*(volatile int*)err || rrqr_now() - t0 > 1000000000ull) {
+        atomicExch(err, 1);
+        break;
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+  return *(volatile int*)err == 0;
+}
+
+// Several independent problems share one cooperative launch: problem p owns
+// the CTAs [start[p], start[p+1]) and runs its phases on them alone; the
+// barriers span the whole grid, so a problem whose partition 2 stops early
+// only waits for the others.
+constexpr int kRRQRFusedMax = 8;
+struct RRQRFusedLayout {
+  int np;
+  int start[kRRQRFusedMax + 1];
+};
+
+__global__ void __launch_bounds__(QR_NT) rrqr_fused_kernel(const RRQRProblem* __restrict__ probs,
+                                                           RRQRFusedLayout lay, int p2steps, unsigned* bar,
+                                                           int* err) {
+  __shared__ double shv[33];
+  __shared__ int shi[33];
+  __shared__ zd s_alpha;
+  int pi = 0;
+  while (pi + 1 < lay.np && (int)blockIdx.x >= lay.start[pi + 1]) ++pi;
+  const RRQRProblem P = probs[pi];
+  const int cta = (int)blockIdx.x - lay.start[pi], nctas = lay.start[pi + 1] - lay.start[pi];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = QR_NT / 32;
+  const int stride = nctas * nw;
+  unsigned target = 0;
+  auto sync = [&]() {
+    target += gridDim.x;
+    if (rrqr_grid_sync(bar, target, err)) return true;
+    if (cta == 0 && threadIdx.x == 0) *P.rank = -2;
+    return false;
+  };
+  if (cta == 0) rrqr_p1_body(P, shv, shi, s_alpha);
+  if (!sync()) return;
+  for (int q = P.partition + cta * nw + warp; q < P.n; q += stride) rrqr_fill_col(P, q, lane);
+  if (!sync()) return;
+  if (cta == 0) rrqr_p2_init_body(P);
+  if (!sync()) return;
+  for (int t = 0; t < p2steps; ++t) {
+    if (cta == 0) rrqr_p2_pivot_body(P, t, shv, shi, s_alpha);
+    if (!sync()) return;
+    const int j = *(volatile int*)&P.istate[6];
+    if (j >= 0)
+      for (int q = j + cta * nw + warp; q < P.n; q += stride) rrqr_p2_apply_col(P, j, q, lane);
+    if (!sync()) return;
+  }
+  if (cta == 0) rrqr_p2_finish_body(P);
+  if (!sync()) return;
+  const int rank = *(volatile int*)&P.istate[3];
+  for (int c = cta * nw + warp; c < rank; c += stride) rrqr_q_col(P, c, lane);
 }
 
 void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
@@ -820,6 +916,47 @@ void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs) {
   }
   DevBuf dp = upload(ctx, probs);
   const unsigned np = (unsigned)probs.size();
+  if (np <= (unsigned)kRRQRFusedMax && p2steps <= kRRQRStepLaunchMax) {  // one cooperative launch
+    // resident CTAs of the fused kernel per SM (a property of the kernel and the architecture)
+    static const int maxPerSM = [] {
+      int v = 0;
+      AIFMM_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, rrqr_fused_kernel, QR_NT, 0));
+      return v;
+    }();
+    const int sms = ctx->numSMs > 0 ? ctx->numSMs : 148;
+    const int resident = sms * maxPerSM;
+    if (maxPerSM > 0 && (int)np <= resident) {
+      // one warp per column: CTAs by column count, scaled down together to what is resident at once
+      std::vector<int> want(np);
+      long total = 0;
+      for (unsigned p = 0; p < np; ++p) {
+        want[p] = std::max((probs[p].n + QR_NT / 32 - 1) / (QR_NT / 32), 1);
+        total += want[p];
+      }
+      RRQRFusedLayout lay{};
+      lay.np = (int)np;
+      int grid = 0;
+      for (unsigned p = 0; p < np; ++p) {
+        int g = want[p];
+        if (total > resident) g = std::max(1, (int)((long)want[p] * (resident - (long)np) / total));
+        lay.start[p] = grid;
+        grid += g;
+      }
+      lay.start[np] = grid;
+      AIFMM_REQUIRE(grid <= resident, AIFMM_EINVAL, "fused RRQR grid exceeds the resident CTAs");
+      DevBuf sync(ctx, 16);
+      AIFMM_CUDA(cudaMemsetAsync(sync.p, 0, 16, ctx->stream));
+      const RRQRProblem* pp = dp.as<RRQRProblem>();
+      unsigned* bar = sync.as<unsigned>();
+      int* err = reinterpret_cast<int*>(sync.as<unsigned>() + 1);
+      int steps = p2steps;
+      void* args[] = {(void*)&pp, (void*)&lay, (void*)&steps, (void*)&bar, (void*)&err};
+      AIFMM_CUDA(cudaLaunchCooperativeKernel((const void*)rrqr_fused_kernel, dim3(grid), dim3(QR_NT), args, 0,
+                                             ctx->stream));
+      AIFMM_LAUNCHED();
+      return;
+    }
+  }
   rrqr_p1_kernel<<<np, QR_NT, 0, ctx->stream>>>(dp.as<RRQRProblem>());
   AIFMM_LAUNCHED();
   rrqr_fill_kernel<<<dim3((maxFill + 7) / 8, np), 256, 0, ctx->stream>>>(dp.as<RRQRProblem>());

@@ -48,10 +48,13 @@ struct RRQRProblem {
 
 // Single-kernel RRQR (one CTA per problem).
 void launch_rrqr(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs);
-// Same factorization in four launches: the partition-1 panel in one CTA,
+// Same factorization split into phases: the partition-1 panel in one CTA,
 // the committed reflectors applied to the fill-in columns one warp per
-// column, the partition-2 steps in one CTA, and Q_trunc one warp per column.
-// Needs istate/dstate; the result equals launch_rrqr's bit for bit.
+// column, the partition-2 steps (pivot in one CTA, the reflector applied one
+// warp per column), and Q_trunc one warp per column.  One problem runs as a
+// single cooperative launch with grid-wide barriers between the phases;
+// several as one launch per phase.  Needs istate/dstate; the result equals
+// launch_rrqr's bit for bit.
 void launch_rrqr_split(aifmm_ctx* ctx, const std::vector<RRQRProblem>& probs);
 
 }  // namespace aifmm

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstring>
 #include <limits>
 
 #include "h2op.cuh"
@@ -570,59 +571,12 @@ bool Solver::wellSeparated(int j, int k, int l) const {  // T:4044-4055
   return true;
 }
 
-// Partitioned column-pivoted QR of the working copy R (destroyed); returns
-// Q_trunc.  p2cap bounds the partition-2 steps (-1: none).
-DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot) {
-  opprof::Scope prof_("rrqr_kernels", ctx->stream);
-  const int m = R.r, n = R.c;
-  const int hs = std::min(m, n) + 1;
-  DevBuf H(ctx, sizeof(zd) * (size_t)m * hs + 16), Q(ctx, sizeof(zd) * (size_t)m * hs + 16);
-  DevBuf nsq(ctx, sizeof(double) * n + 8), perm(ctx, sizeof(int) * n + 8), out(ctx, 64);
-  RRQRProblem P;
-  P.R = R.p;
-  P.m = m;
-  P.n = n;
-  P.partition = partition;
-  P.tol1 = std::pow(10.0, -prm.tol_pow);
-  P.tol2 = std::pow(10.0, -prm.fillin_tol);
-  P.inputPivot = inputPivot;
-  P.fillInRank = fillRank;
-  P.realMode = prm.realMode;
-  P.H = H.as<zd>();
-  P.nsq = nsq.as<double>();
-  P.perm = perm.as<int>();
-  P.Q = Q.as<zd>();
-  P.rank = (int*)out.p;
-  P.maxPivot = (double*)((char*)out.p + 8);
-  P.istate = (int*)((char*)out.p + 16);
-  P.dstate = (double*)((char*)out.p + 48);  // after the 8 ints of istate
-  P.p2cap = p2cap;
-  cudaEvent_t e0 = nullptr, e1 = nullptr;
-  if (gemm_profile_on()) {
-    AIFMM_CUDA(cudaEventCreate(&e0));
-    AIFMM_CUDA(cudaEventCreate(&e1));
-    AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
-  }
-  launch_rrqr_split(ctx, {P});
-  if (gemm_profile_on()) {
-    AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
-    device_span_record(e0, e1, "rrqr:" + opprof::path(), 0.0);
-  }
-  stats.kernels += 4;
-  struct {
-    int rank, pad;
-    double mp;
-  } h;
-  AIFMM_CUDA(cudaMemcpyAsync(&h, out.p, 16, cudaMemcpyDeviceToHost, ctx->stream));
-  ops.sync();
-  AIFMM_REQUIRE(h.rank >= 0 && h.rank <= std::min(m, n), AIFMM_EINVAL, "RRQR rank out of range");
-  maxPivot = h.mp;
-  DMat Qt = ops.alloc(m, h.rank);
-  if (Qt.size()) AIFMM_CUDA(cudaMemcpyAsync(Qt.p, Q.p, sizeof(zd) * Qt.size(), cudaMemcpyDeviceToDevice, ctx->stream));
-  return Qt;
-}
-
-// RRQR of A = [old basis (partition columns) | fill-in] (rrqr.cpp:98-182).
+// RRQR of A = [old basis (partition columns) | fill-in] (rrqr.cpp:98-182),
+// for several independent matrices at once: one launch of the column-pivoted
+// QR kernels for all of them and one read-back of their ranks, where one
+// call each would pay a launch chain and a host round trip apiece.  Each
+// matrix's arithmetic is that of a call on its own, bit for bit.
+//
 // When the old basis has orthonormal columns (orthoPanel), partition 1 of the
 // reference keeps every one of them -- each pivot is the unit norm of a
 // column orthogonal to the ones before, never below tol1 <= 1 -- so its
@@ -633,39 +587,125 @@ DMat Solver::rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int
 // pivots and spans are those of the full pass, the basis of the old span is
 // the identity instead of a Householder rotation of it, and maxPivot of an
 // empty partition 2 is the unit norm of the first old column.
-DMat Solver::rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel,
-                  bool* prefix) {
+void Solver::rrqrBatch(const std::vector<RRQRJob*>& jobs) {
   opprof::Scope prof_fn_("rrqr_total", ctx->stream);
   PhaseTimer pt(*this, stats.t_rrqr);
-  const int m = A.r, n = A.c;
-  stats.nRRQR++;
-  if (prefix) *prefix = false;
-  if (!(orthoPanel && prm.orthoShortcut && partition > 0 && partition <= m))
-    return rrqrRun(ops.copy(A), partition, inputPivot, fillRank, -1, maxPivot);
-  stats.nRRQRShort++;
-  if (prefix) *prefix = true;  // Q_trunc = [old basis | new columns]
-  const int r = partition, nf = n - partition;
-  DMat Q1;  // view of the old basis
-  Q1.buf = A.buf;
-  Q1.p = A.p;
-  Q1.r = m;
-  Q1.c = r;
-  if (nf == 0 || m == r) {
-    maxPivot = 1.0;
-    return ops.copy(Q1);
+  struct Run {
+    RRQRJob* job;
+    DMat R;       // working copy, destroyed
+    int partition, p2cap;
+    DMat Q1;      // shortcut: view of the old basis
+    bool shortcut;
+  };
+  std::vector<Run> runs;
+  for (RRQRJob* J : jobs) {
+    const int m = J->A.r, n = J->A.c;
+    stats.nRRQR++;
+    J->prefix = false;
+    if (!(J->orthoPanel && prm.orthoShortcut && J->partition > 0 && J->partition <= m)) {
+      runs.push_back({J, ops.copy(J->A), J->partition, -1, DMat(), false});
+      continue;
+    }
+    stats.nRRQRShort++;
+    J->prefix = true;  // Q_trunc = [old basis | new columns]
+    const int r = J->partition, nf = n - r;
+    DMat Q1;
+    Q1.buf = J->A.buf;
+    Q1.p = J->A.p;
+    Q1.r = m;
+    Q1.c = r;
+    if (nf == 0 || m == r) {
+      J->maxPivot = 1.0;
+      J->Q = ops.copy(Q1);
+      continue;
+    }
+    DMat F = ops.block(J->A, 0, r, m, nf);
+    // classical Gram-Schmidt twice: the second pass restores orthogonality to
+    // rounding.  One pass is not enough even for the mixed path's
+    // preconditioner: a fill-in mostly inside the old span leaves a small
+    // remainder whose non-orthogonal part the normalisation amplifies, and
+    // the partial-identity basis changes assume orthonormal columns.
+    for (int pass = 0; pass < 2; ++pass) {
+      const DMat C = ops.mul(Q1, OP_C, F, OP_N);
+      GemmBatch g;
+      g.add(F, Q1, OP_N, C, OP_N, MONE, ONE);
+      g.flush(ctx);
+    }
+    runs.push_back({J, F, 0, m - r, Q1, true});
   }
-  DMat F = ops.block(A, 0, r, m, nf);
-  for (int pass = 0; pass < 2; ++pass) {
-    const DMat C = ops.mul(Q1, OP_C, F, OP_N);
-    GemmBatch g;
-    g.add(F, Q1, OP_N, C, OP_N, MONE, ONE);
-    g.flush(ctx);
+  if (runs.empty()) return;
+  opprof::Scope prof_("rrqr_kernels", ctx->stream);
+  constexpr size_t kOut = 64;  // rank, maxPivot, istate[8], dstate[2] of one problem
+  DevBuf out(ctx, kOut * runs.size());
+  std::vector<DevBuf> H(runs.size()), Q(runs.size()), nsq(runs.size()), perm(runs.size());
+  std::vector<RRQRProblem> probs(runs.size());
+  for (size_t i = 0; i < runs.size(); ++i) {
+    const Run& u = runs[i];
+    const int m = u.R.r, n = u.R.c;
+    const int hs = std::min(m, n) + 1;
+    H[i].alloc(ctx, sizeof(zd) * (size_t)m * hs + 16);
+    Q[i].alloc(ctx, sizeof(zd) * (size_t)m * hs + 16);
+    nsq[i].alloc(ctx, sizeof(double) * n + 8);
+    perm[i].alloc(ctx, sizeof(int) * n + 8);
+    char* o = (char*)out.p + kOut * i;
+    RRQRProblem& P = probs[i];
+    P.R = u.R.p;
+    P.m = m;
+    P.n = n;
+    P.partition = u.partition;
+    P.tol1 = std::pow(10.0, -prm.tol_pow);
+    P.tol2 = std::pow(10.0, -prm.fillin_tol);
+    P.inputPivot = u.job->inputPivot;
+    P.fillInRank = u.job->fillRank;
+    P.realMode = prm.realMode;
+    P.H = H[i].as<zd>();
+    P.nsq = nsq[i].as<double>();
+    P.perm = perm[i].as<int>();
+    P.Q = Q[i].as<zd>();
+    P.rank = (int*)o;
+    P.maxPivot = (double*)(o + 8);
+    P.istate = (int*)(o + 16);
+    P.dstate = (double*)(o + 48);  // after the 8 ints of istate
+    P.p2cap = u.p2cap;
   }
-  const DMat Q2 = rrqrRun(F, 0, inputPivot, fillRank, m - r, maxPivot);
-  DMat Qt = ops.alloc(m, r + Q2.c);
-  zcopy_grouped(ctx, {{Q1.p, Qt.p, m, r, Q1.ld(), Qt.ld(), 0, ONE},
-                      {Q2.p, Qt.p + (size_t)r * Qt.ld(), m, Q2.c, Q2.ld(), Qt.ld(), 0, ONE}});
-  return Qt;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (gemm_profile_on()) {
+    AIFMM_CUDA(cudaEventCreate(&e0));
+    AIFMM_CUDA(cudaEventCreate(&e1));
+    AIFMM_CUDA(cudaEventRecord(e0, ctx->stream));
+  }
+  launch_rrqr_split(ctx, probs);
+  if (gemm_profile_on()) {
+    AIFMM_CUDA(cudaEventRecord(e1, ctx->stream));
+    device_span_record(e0, e1, "rrqr:" + opprof::path(), 0.0);
+  }
+  stats.kernels += 4 * (long)runs.size();
+  std::vector<char> h(kOut * runs.size());
+  AIFMM_CUDA(cudaMemcpyAsync(h.data(), out.p, h.size(), cudaMemcpyDeviceToHost, ctx->stream));
+  ops.sync();
+  std::vector<CopyProblem> cps;
+  for (size_t i = 0; i < runs.size(); ++i) {
+    const Run& u = runs[i];
+    RRQRJob* J = u.job;
+    const int m = u.R.r, n = u.R.c;
+    int rank;
+    double mp;
+    std::memcpy(&rank, h.data() + kOut * i, sizeof(int));
+    std::memcpy(&mp, h.data() + kOut * i + 8, sizeof(double));
+    AIFMM_REQUIRE(rank != -2, AIFMM_ETIMEOUT, "RRQR: a bounded grid-barrier wait ran out");
+    AIFMM_REQUIRE(rank >= 0 && rank <= std::min(m, n), AIFMM_EINVAL, "RRQR rank out of range");
+    J->maxPivot = mp;
+    if (!u.shortcut) {
+      J->Q = ops.alloc(m, rank);
+      if (rank > 0) cps.push_back({Q[i].as<zd>(), J->Q.p, m, rank, m, J->Q.ld(), 0, ONE});
+    } else {
+      const int r = u.Q1.c;
+      J->Q = ops.alloc(m, r + rank);
+      cps.push_back({u.Q1.p, J->Q.p, m, r, u.Q1.ld(), J->Q.ld(), 0, ONE});
+      if (rank > 0) cps.push_back({Q[i].as<zd>(), J->Q.p + (size_t)r * J->Q.ld(), m, rank, m, J->Q.ld(), 0, ONE});
+    }
+  }
+  zcopy_grouped(ctx, cps);
 }
 
 void Solver::resizeRows(const std::vector<DMat*>& blocks, int rows) {
@@ -799,16 +839,11 @@ void Solver::updateParentP2M(int j, int b, const DMat& nP2Mt, bool prefix) {  //
   tree[j - 1][bP].p2mOrtho = false;
 }
 
-void Solver::compressP2PRRQR(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& P2Pt,
-                             DMat& nL2P, DMat& nP2Mt, DMat& newM2L, bool& prefixL, bool& prefixM) {  // T:1573-1656
-  double mp1, mp2;
-  nL2P = rrqr(ops.hcat(oldL2P, P2Pt), oldL2P.c, tree[j][k].maxPivot_L2P, fillin_rankVec[j], mp1, tree[j][k].l2pOrtho,
-              &prefixL);
-  tree[j][k].maxPivot_L2P = std::max(tree[j][k].maxPivot_L2P, mp1);
-  const DMat Rkp = ops.mul(nL2P, OP_C, P2Pt, OP_N);
-  nP2Mt = rrqr(ops.hcat(ops.adj(oldP2M), ops.adj(Rkp)), oldP2M.r, tree[j][b].maxPivot_P2M, fillin_rankVec[j], mp2,
-               tree[j][b].p2mOrtho, &prefixM);
-  tree[j][b].maxPivot_P2M = std::max(tree[j][b].maxPivot_P2M, mp2);
+// The new M2L block of compressP2P_myRRQR (T:1573-1656) once its two RRQRs
+// gave the new bases: Rnp^H from the projected fill-in Rkp = nL2P^H P2Pt,
+// plus the old M2L block carried into the new bases.
+void Solver::compressP2PM2L(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& nL2P,
+                            const DMat& nP2Mt, const DMat& Rkp, DMat& newM2L, bool prefixL, bool prefixM) {
   const DMat Rnp = ops.mul(nP2Mt, OP_C, Rkp, OP_C);
   newM2L = ops.adj(Rnp);
   DMat& M = tree[j][k].M2L[b];
@@ -855,13 +890,51 @@ void Solver::compressP2PTwoWays(int j, int k, int b) {  // T:2116-2306
   DMat nL2P_k, nP2Mt_b, M2L_k_b, nL2P_b, nP2Mt_k, M2L_b_k;
   bool pkL, pbM, pbL, pkM;  // which new bases start with the old ones
   {
-  opprof::Scope prof_fn_("compress_p2p", ctx->stream);
-    DMat a = tree[j][k].L2P, bb = tree[j][b].P2M, c = tree[j][k].P2P[b];
-    compressP2PRRQR(j, k, b, a, bb, c, nL2P_k, nP2Mt_b, M2L_k_b, pkL, pbM);
-  }
-  {
-    DMat a = tree[j][b].L2P, bb = tree[j][k].P2M, c = tree[j][b].P2P[k];
-    compressP2PRRQR(j, b, k, a, bb, c, nL2P_b, nP2Mt_k, M2L_b_k, pbL, pkM);
+    opprof::Scope prof_fn_("compress_p2p", ctx->stream);
+    // compressP2P_myRRQR(j, k, b) and (j, b, k) side by side: the two
+    // directions read disjoint bases and blocks, so their row-basis RRQRs run
+    // as one batch, then their column-basis RRQRs
+    const DMat Lk = tree[j][k].L2P, Mb = tree[j][b].P2M, Pkb = tree[j][k].P2P[b];
+    const DMat Lb = tree[j][b].L2P, Mk = tree[j][k].P2M, Pbk = tree[j][b].P2P[k];
+    RRQRJob r1, r3;
+    r1.A = ops.hcat(Lk, Pkb);
+    r1.partition = Lk.c;
+    r1.inputPivot = tree[j][k].maxPivot_L2P;
+    r1.fillRank = fillin_rankVec[j];
+    r1.orthoPanel = tree[j][k].l2pOrtho;
+    r3.A = ops.hcat(Lb, Pbk);
+    r3.partition = Lb.c;
+    r3.inputPivot = tree[j][b].maxPivot_L2P;
+    r3.fillRank = fillin_rankVec[j];
+    r3.orthoPanel = tree[j][b].l2pOrtho;
+    rrqrBatch({&r1, &r3});
+    nL2P_k = r1.Q;
+    pkL = r1.prefix;
+    tree[j][k].maxPivot_L2P = std::max(tree[j][k].maxPivot_L2P, r1.maxPivot);
+    nL2P_b = r3.Q;
+    pbL = r3.prefix;
+    tree[j][b].maxPivot_L2P = std::max(tree[j][b].maxPivot_L2P, r3.maxPivot);
+    const DMat Rkp = ops.mul(nL2P_k, OP_C, Pkb, OP_N), Rbp = ops.mul(nL2P_b, OP_C, Pbk, OP_N);
+    RRQRJob r2, r4;
+    r2.A = ops.hcat(ops.adj(Mb), ops.adj(Rkp));
+    r2.partition = Mb.r;
+    r2.inputPivot = tree[j][b].maxPivot_P2M;
+    r2.fillRank = fillin_rankVec[j];
+    r2.orthoPanel = tree[j][b].p2mOrtho;
+    r4.A = ops.hcat(ops.adj(Mk), ops.adj(Rbp));
+    r4.partition = Mk.r;
+    r4.inputPivot = tree[j][k].maxPivot_P2M;
+    r4.fillRank = fillin_rankVec[j];
+    r4.orthoPanel = tree[j][k].p2mOrtho;
+    rrqrBatch({&r2, &r4});
+    nP2Mt_b = r2.Q;
+    pbM = r2.prefix;
+    tree[j][b].maxPivot_P2M = std::max(tree[j][b].maxPivot_P2M, r2.maxPivot);
+    nP2Mt_k = r4.Q;
+    pkM = r4.prefix;
+    tree[j][k].maxPivot_P2M = std::max(tree[j][k].maxPivot_P2M, r4.maxPivot);
+    compressP2PM2L(j, k, b, Lk, Mb, nL2P_k, nP2Mt_b, Rkp, M2L_k_b, pkL, pbM);
+    compressP2PM2L(j, b, k, Lb, Mk, nL2P_b, nP2Mt_k, Rbp, M2L_b_k, pbL, pkM);
   }
   DMat kL, kM, bL, bM;
   equalise(ops, nL2P_k, nP2Mt_k, kL, kM);
@@ -897,12 +970,28 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
   PhaseTimer pt(*this, stats.t_compress);
   stats.nCompressP2L++;
   DBox& Bk = tree[j][k];
+  DBox& Bb = tree[j][b];
+  // the RRQRs of compress_M2P_myRRQR(j, k, b) (A = [L2P_k | M2P[b]]) and of
+  // compress_P2L_myRRQR(j, b, k) (A_row = [P2M_k^H | P2L[b][k]^H]) read
+  // disjoint blocks: one batch
+  RRQRJob rl, rm;
+  rl.A = ops.hcat(Bk.L2P, Bk.M2P[b]);
+  rl.partition = Bk.L2P.c;
+  rl.inputPivot = Bk.maxPivot_L2P;
+  rl.fillRank = fillin_rankVec[j];
+  rl.orthoPanel = Bk.l2pOrtho;
+  rm.A = ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k]));
+  rm.partition = Bk.P2M.r;
+  rm.inputPivot = Bk.maxPivot_P2M;
+  rm.fillRank = fillin_rankVec[j];
+  rm.orthoPanel = Bk.p2mOrtho;
+  rrqrBatch({&rl, &rm});
+  const bool pL = rl.prefix, pM = rm.prefix;  // the new bases start with the old ones
+  DMat nL2P_k = rl.Q;
+  Bk.maxPivot_L2P = std::max(Bk.maxPivot_L2P, rl.maxPivot);
+  DMat nP2Mt_k = rm.Q;
+  Bk.maxPivot_P2M = std::max(Bk.maxPivot_P2M, rm.maxPivot);
   // compress_M2P_myRRQR(j, k, b)
-  double mp;
-  bool pL = false, pM = false;  // the new bases start with the old ones
-  DMat nL2P_k =
-      rrqr(ops.hcat(Bk.L2P, Bk.M2P[b]), Bk.L2P.c, Bk.maxPivot_L2P, fillin_rankVec[j], mp, Bk.l2pOrtho, &pL);
-  Bk.maxPivot_L2P = std::max(Bk.maxPivot_L2P, mp);
   DMat M2L_k_b = ops.mul(nL2P_k, OP_C, Bk.M2P[b], OP_N);  // Rk'
   {
   opprof::Scope prof_fn_("compress_p2l", ctx->stream);
@@ -918,11 +1007,7 @@ void Solver::compressM2PP2L(int j, int k, int b) {  // T:2454-2596, :2878-2959
       g.flush(ctx);
     }
   }
-  // compress_P2L_myRRQR(j, b, k): A_row = [P2M_k^H | P2L[b][k]^H]
-  DBox& Bb = tree[j][b];
-  DMat nP2Mt_k = rrqr(ops.hcat(ops.adj(Bk.P2M), ops.adj(Bb.P2L[k])), Bk.P2M.r, Bk.maxPivot_P2M, fillin_rankVec[j], mp,
-                      Bk.p2mOrtho, &pM);
-  Bk.maxPivot_P2M = std::max(Bk.maxPivot_P2M, mp);
+  // compress_P2L_myRRQR(j, b, k)
   DMat M2L_b_k;
   {
     const DMat Rnp = ops.mul(nP2Mt_k, OP_C, Bb.P2L[k], OP_C);
@@ -1232,6 +1317,7 @@ void Solver::factorize() {  // eliminate_phase_efficient, T:4599-4747
   const double t0 = wall();
   AIFMM_CUDA(cudaSetDevice(ctx->device));
   const long tc0 = prm.precision >= 2 ? tc_timeouts() : 0;
+  dropPlan();  // its graph reads the blocks this factorization replaces
   stats.nRRQR = stats.nRRQRShort = stats.nCompressP2P = stats.nCompressP2L = 0;
   // A fresh tree's fill-in queues are empty.  The reference does not clear
   // them between levels, and pairs queued late at one level can still be
@@ -1459,10 +1545,78 @@ void Solver::backSubstitute() {  // back_substitution_phase, T:4812-4865
     }
 }
 
+SolvePlan::~SolvePlan() {
+  if (ctx) cudaStreamSynchronize(ctx->stream);  // no replay in flight
+  if (exec) cudaGraphExecDestroy(exec);
+  if (graph) cudaGraphDestroy(graph);
+  if (hold) hold->releaseAll();
+}
+
+// Captures solveSweeps(in) -> out on the context stream.  During the capture
+// the context allocates and uploads outside it (aifmm_ctx::capture), so the
+// graph holds only kernels, memsets and device-to-device copies; the kernel
+// launches counted while capturing are not launches and are taken back.
+void Solver::capturePlan(int nrhs) {
+  opprof::Scope prof_fn_("solve_capture", ctx->stream);
+  plan_.reset();
+  treeOrder();
+  std::unique_ptr<SolvePlan> pl(new SolvePlan);
+  pl->ctx = ctx;
+  pl->nrhs = nrhs;
+  pl->in = ops.alloc(N, nrhs);
+  pl->out = ops.alloc(N, nrhs);
+  pl->hold = std::make_shared<CaptureHold>();
+  pl->hold->ctx = ctx;
+  if (!ctx->sideStream) AIFMM_CUDA(cudaStreamCreateWithFlags(&ctx->sideStream, cudaStreamNonBlocking));
+  AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
+  const long l0 = launch_count();
+  AIFMM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+  ctx->capture = pl->hold;
+  try {
+    const DMat x = solveSweeps(pl->in);
+    AIFMM_CUDA(cudaMemcpyAsync(pl->out.p, x.p, sizeof(zd) * x.size(), cudaMemcpyDeviceToDevice, ctx->stream));
+  } catch (...) {
+    ctx->capture.reset();
+    cudaGraph_t g = nullptr;
+    cudaStreamEndCapture(ctx->stream, &g);
+    if (g) cudaGraphDestroy(g);
+    cudaGetLastError();
+    count_launch(l0 - launch_count());
+    throw;
+  }
+  ctx->capture.reset();
+  const cudaError_t e = cudaStreamEndCapture(ctx->stream, &pl->graph);
+  pl->launches = launch_count() - l0;
+  count_launch(-pl->launches);
+  AIFMM_CUDA(e);
+  AIFMM_CUDA(cudaGraphInstantiate(&pl->exec, pl->graph, 0));
+  stats.nSolveCapture++;
+  plan_ = std::move(pl);
+}
+
 DMat Solver::solve(const DMat& rhs) {
   AIFMM_REQUIRE(factored, AIFMM_ESTATE, "solve before factorize");
   AIFMM_REQUIRE(rhs.r == N && rhs.c >= 1, AIFMM_EINVAL, "rhs must be N x nrhs");
   const double t0 = wall();
+  // the per-launch profilers time each launch with host synchronisation: eager sweeps
+  if (graphSolve && !opprof::enabled() && !gemm_profile_on()) {
+    if (!plan_ || plan_->nrhs != rhs.c) capturePlan(rhs.c);
+    AIFMM_CUDA(cudaMemcpyAsync(plan_->in.p, rhs.p, sizeof(zd) * rhs.size(), cudaMemcpyDeviceToDevice, ctx->stream));
+    AIFMM_CUDA(cudaGraphLaunch(plan_->exec, ctx->stream));
+    count_launch(plan_->launches);
+    DMat x = ops.copy(plan_->out);
+    ops.sync();
+    stats.nSolveGraph++;
+    stats.t_solve = wall() - t0;
+    return x;
+  }
+  DMat x = solveSweeps(rhs);
+  ops.sync();
+  stats.t_solve = wall() - t0;
+  return x;
+}
+
+DMat Solver::solveSweeps(const DMat& rhs) {
   nrhs_ = rhs.c;
   assignLeafRhs(rhs);
   // rhs_eliminate_phase_efficient, T:4749-4770
@@ -1495,8 +1649,6 @@ DMat Solver::solve(const DMat& rhs) {
   zcopy_grouped(ctx, cps);
   DMat x = ops.alloc(N, nrhs_);
   zrows_scatter(ctx, Yt.p, Yt.ld(), leafPerm_->as<int>(), N, x.p, x.ld(), nrhs_);
-  ops.sync();
-  stats.t_solve = wall() - t0;
   return x;
 }
 
@@ -1536,6 +1688,8 @@ void Solver::checkpoint() {
 
 void Solver::rewind() {
   AIFMM_REQUIRE(hasSaved_, AIFMM_ESTATE, "no checkpoint to rewind to");
+  dropPlan();
+  tree.clear();  // the factorized blocks go before the copy is made: one tree's memory less at the peak
   tree = deepCopy(saved_);
   P2Pq.clear();
   P2L_M2P.clear();

@@ -33,6 +33,7 @@ struct SolverStats {
   double flops_factor = 0;  // complex-counted algorithmic flops issued by the factorization
   long nRRQR = 0, nRRQRShort = 0, nCompressP2P = 0, nCompressP2L = 0, nACA = 0, nACARetry = 0;
   long kernels = 0;
+  long nSolveGraph = 0, nSolveCapture = 0;  // solves replayed from a captured graph / graphs captured
   double t_aca = 0;          // host time of the ACA phase (launches, retries, read-backs)
   double aca_ws_bytes = 0;   // ACA workspace bytes allocated over all launches (retries included)
   long nACALaunches = 0;     // ACA launches (chunks of problems that fit the workspace budget)
@@ -43,6 +44,22 @@ struct SolverStats {
 struct ACARecord {
   RankFeatures x;
   int rmax0, rank;
+};
+
+// A captured CUDA graph of the whole solve sweep for one right-hand-side
+// count: it reads `in` and writes `out`, buffers of the plan, and every
+// intermediate block it touches stays reserved by `hold` while it exists.
+// The graph's kernels read the factorization's blocks at their addresses, so
+// a plan is dropped whenever they change (factorize, rewind, load).
+struct SolvePlan {
+  aifmm_ctx* ctx = nullptr;
+  int nrhs = 0;
+  DMat in, out;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  std::shared_ptr<CaptureHold> hold;
+  long launches = 0;  // kernels per replay
+  ~SolvePlan();
 };
 
 struct DBox {
@@ -93,8 +110,14 @@ class Solver {
   Solver(aifmm_kernel* k, const SolverParams& p, const double* xyz = nullptr, const double* dom = nullptr);
   void build();
   void factorize();
-  // rhs: N x nrhs (device), returns x: N x nrhs (device)
+  // rhs: N x nrhs (device), returns x: N x nrhs (device).  With graphSolve
+  // (the default) the first solve for a right-hand-side count after a
+  // factorization captures the sweep as a CUDA graph and every solve,
+  // that one included, replays it: one graph launch instead of thousands of
+  // kernel launches issued from the host.
   DMat solve(const DMat& rhs);
+  bool graphSolve = true;
+  void dropPlan() { plan_.reset(); }  // the next solve captures again
 
   int avgLeafSize() const;
   int avgMultipoles() const;
@@ -127,8 +150,9 @@ class Solver {
   void eliminateX(int j, int k);
   void eliminateZ(int j, int k);
   void compressP2PTwoWays(int j, int k, int b);
-  void compressP2PRRQR(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& P2Pt, DMat& nL2P,
-                       DMat& nP2Mt, DMat& newM2L, bool& prefixL, bool& prefixM);
+  // newM2L of compressP2P_myRRQR from the new bases (the products after its two RRQRs)
+  void compressP2PM2L(int j, int k, int b, const DMat& oldL2P, const DMat& oldP2M, const DMat& nL2P,
+                      const DMat& nP2Mt, const DMat& Rkp, DMat& newM2L, bool prefixL, bool prefixM);
   void compressM2PP2L(int j, int k, int b);
   // prefix: the new basis starts with the old one (the RRQR kept an
   // orthonormal old basis), so the basis change is a partial identity and
@@ -141,9 +165,21 @@ class Solver {
   // (first columns kept, zero right); one grouped copy for all of them
   void resizeRows(const std::vector<DMat*>& blocks, int rows);
   void resizeCols(const std::vector<DMat*>& blocks, int cols);
-  DMat rrqr(const DMat& A, int partition, double inputPivot, int fillRank, double& maxPivot, bool orthoPanel,
-            bool* prefix = nullptr);
-  DMat rrqrRun(DMat R, int partition, double inputPivot, int fillRank, int p2cap, double& maxPivot);
+  // One recompression RRQR: A = [old basis (partition columns) | fill-in].
+  struct RRQRJob {
+    DMat A;
+    int partition = 0;
+    double inputPivot = 0;
+    int fillRank = 0;
+    bool orthoPanel = false;  // the old basis has orthonormal columns
+    DMat Q;                   // out: Q_trunc
+    double maxPivot = 0;      // out
+    bool prefix = false;      // out: Q starts with the old basis
+  };
+  void rrqrBatch(const std::vector<RRQRJob*>& jobs);  // independent jobs, one launch
+  DMat solveSweeps(const DMat& rhs);  // the sweep, enqueued without synchronising
+  void capturePlan(int nrhs);
+  std::unique_ptr<SolvePlan> plan_;
   void assignLeafRhs(const DMat& rhs);
   void rhsEliminateX(int j, int k);
   void rhsEliminateZ(int j, int k);

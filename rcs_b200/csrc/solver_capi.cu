@@ -110,6 +110,14 @@ int aifmm_solver_solve(aifmm_solver* s, const double* rhs, int nrhs, double* x) 
   API_END
 }
 
+int aifmm_solver_set_graph_solve(aifmm_solver* s, int on) {
+  API_BEGIN
+  AIFMM_REQUIRE(s && (on == 0 || on == 1), AIFMM_EINVAL, "bad argument");
+  s->s->graphSolve = on == 1;
+  if (!on) s->s->dropPlan();
+  API_END
+}
+
 int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
   API_BEGIN
   AIFMM_REQUIRE(s && info, AIFMM_EINVAL, "NULL argument");
@@ -126,6 +134,8 @@ int aifmm_solver_get_info(aifmm_solver* s, aifmm_solver_info* info) {
   info->n_aca = S.stats.nACA;
   info->n_aca_retry = S.stats.nACARetry;
   info->kernels = S.stats.kernels;
+  info->n_solve_graph = S.stats.nSolveGraph;
+  info->n_solve_capture = S.stats.nSolveCapture;
   info->t_assemble = S.stats.t_assemble;
   info->t_factor = S.stats.t_factor;
   info->t_solve = S.stats.t_solve;

@@ -208,6 +208,7 @@ void Solver::save(const std::string& path) {
 
 void Solver::load(const std::string& path) {
   AIFMM_CUDA(cudaSetDevice(ctx->device));
+  dropPlan();
   Reader r(path, ctx, ops);
   char magic[8];
   r.raw(magic, 8);

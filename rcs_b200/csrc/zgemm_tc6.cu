@@ -449,6 +449,18 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
       const int row = tm * T6_M + quarter * 32 + lane;
       const uint32_t base = tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * T6_N);
       for (int c0 = 0; c0 < T6_NC; c0 += 16) {
+        // the chunk's 16 C entries of this row are loaded first, all in
+        // flight at once (a warp reads 512 contiguous bytes per column), so
+        // the accumulating tiles pay one memory latency per chunk instead
+        // of one per column
+        zd cv[16];
+        const int ncol = min(16, P.n - (tn * T6_NC + c0));
+        if (!beta0 && row < P.m) {
+          const zd* cp0 = P.C + (size_t)(tn * T6_NC + c0) * P.ldc + row;
+#pragma unroll
+          for (int j = 0; j < 16; ++j)
+            if (j < ncol) cv[j] = __ldcg(cp0 + (size_t)j * P.ldc);
+        }
         uint32_t vr[16], vi[16];
         if (any) {
           asm volatile(
@@ -471,14 +483,13 @@ __global__ void __launch_bounds__(T6_THREADS, 1) zgemm_tc6_kernel(const __grid_c
           for (int j = 0; j < 16; ++j) vr[j] = vi[j] = 0u;
         }
         if (row < P.m) {
+          zd* cp0 = P.C + (size_t)(tn * T6_NC + c0) * P.ldc + row;
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
-            const int col = tn * T6_NC + c0 + j;
-            if (col >= P.n) break;
-            zd* cp = P.C + (size_t)col * P.ldc + row;
+            if (j >= ncol) break;
             zd v = zmul(P.alpha, zmk((double)__uint_as_float(vr[j]), (double)__uint_as_float(vi[j])));
-            if (!beta0) v = zadd(v, zmul(P.beta, *cp));
-            *cp = v;
+            if (!beta0) v = zadd(v, zmul(P.beta, cv[j]));
+            cp0[(size_t)j * P.ldc] = v;
           }
         }
       }

@@ -38,6 +38,16 @@ class Context:
         row-major, 1 column-major) of GEMM precision 4 on this context."""
         _lib.check(_lib.lib().aifmm_ctx_set_gemm_tiling(self.h, int(form), int(raster)))
 
+    def memory(self) -> dict:
+        """Bytes held by the context's buffers (live) and by its memory pool (reserved)."""
+        live, res = C.c_size_t(), C.c_size_t()
+        _lib.check(_lib.lib().aifmm_ctx_memory(self.h, C.byref(live), C.byref(res)))
+        return {"live": live.value, "reserved": res.value}
+
+    def trim(self) -> None:
+        """Return the context's unused device memory (free arena chunks, pooled blocks) to the device."""
+        _lib.check(_lib.lib().aifmm_ctx_trim(self.h))
+
     def tune_report(self) -> list[str]:
         """The GEMM autotuner's trials on this context, one line per launch
         class (GEMM precision 5)."""

@@ -99,6 +99,10 @@ class AIFMM:
         Xm = X.reshape(nrhs, self.N).T
         return Xm[:, 0].copy() if one else Xm.copy()
 
+    def set_graph_solve(self, on: bool) -> None:
+        """Replay solves from a captured CUDA graph of the sweep (True, the default) or issue them launch by launch."""
+        _lib.check(_lib.lib().aifmm_solver_set_graph_solve(self.h, 1 if on else 0))
+
     def solve_device(self, rhs_ptr: int, nrhs: int, x_ptr: int) -> None:
         _lib.check(_lib.lib().aifmm_solver_solve_device(self.h, C.c_void_p(rhs_ptr), int(nrhs), C.c_void_p(x_ptr)))
 

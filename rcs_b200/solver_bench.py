@@ -4,6 +4,7 @@
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
                                     [--precision 0-4] [--drop-pow 0] [--op-tol 10] [--nrhs 8]
                                     [--gmres 1e-6] [--profile-ops] [--profile-host] [--profile-gemm]
+                                    [--profiler-range]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
 AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
@@ -12,7 +13,10 @@ prints one JSON line with the solver's phase timers.  A small, single-pass
 workload for profiling the whole path (for example under a kernel profiler).
 --profile-ops repeats the factorization and the solve with the library's
 per-operation accounting on (every accounted operation then synchronises) and
-prints its table.
+prints its table.  --profiler-range brackets the timed factorization and
+solve with cudaProfilerStart/Stop, so that a kernel profiler run with
+capture from start off (ncu --profile-from-start off) records exactly their
+launches.
 """
 from __future__ import annotations
 
@@ -43,6 +47,8 @@ def main():
                     help="device time of the factorization's GEMM launches and RRQR chains by call site")
     ap.add_argument("--profile-host", action="store_true",
                     help="time the factorization with host-only accounting (no extra synchronisation)")
+    ap.add_argument("--profiler-range", action="store_true",
+                    help="cudaProfilerStart/Stop around the timed factorization and solve")
     a = ap.parse_args()
     from . import mesh as M
     from .kernel import EFIEMatrix
@@ -64,6 +70,10 @@ def main():
     if a.profile_gemm:
         from .solver import profile_gemm
         profile_gemm(True)
+    if a.profiler_range:
+        import torch
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
     t0 = time.perf_counter()
     S.factorize()
     t_fac = time.perf_counter() - t0
@@ -91,6 +101,9 @@ def main():
     else:
         X = S.solve(B)
     t_sol = time.perf_counter() - t0
+    if a.profiler_range:
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
     info = S.info()
     if a.precision == 5:
         for line in K.ctx.tune_report():

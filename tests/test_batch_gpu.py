@@ -29,7 +29,8 @@ def test_batch_equals_one_by_one(precision):
     rhs = [rng.standard_normal((K.N, 2)) + 1j * rng.standard_normal((K.N, 2)) for _, K, _ in bodies]
     for _, _, S in bodies:
         S.checkpoint()
-    for _, _, S in bodies:
+    for _, _, S in bodies:  # one by one, from the checkpoint (the batch's starting point)
+        S.rewind()
         S.factorize()
     single = [S.solve(b) for (_, _, S), b in zip(bodies, rhs)]
     for _, _, S in bodies:
