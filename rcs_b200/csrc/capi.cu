@@ -17,8 +17,13 @@ namespace aifmm {
 static thread_local std::string g_last_error;
 void set_last_error(const std::string& msg) { g_last_error = msg; }
 static std::atomic<long> g_launches{0};
-void count_launch(long n) { g_launches += n; }
+static thread_local long t_launches = 0;
+void count_launch(long n) {
+  g_launches += n;
+  t_launches += n;
+}
 long launch_count() { return g_launches.load(); }
+long thread_launch_count() { return t_launches; }
 
 static std::mutex g_ctx_mu;
 

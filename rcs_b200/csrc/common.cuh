@@ -26,6 +26,9 @@ void smem_attr_once(const void* kernel, int device, int bytes);
 // Number of kernels this library has launched (all contexts, process-wide).
 void count_launch(long n = 1);
 long launch_count();
+// The launches counted on the calling thread only (for a thread's own
+// before/after differences while other threads launch too).
+long thread_launch_count();
 
 #define AIFMM_CUDA(expr)                                                                                  \
   do {                                                                                                    \

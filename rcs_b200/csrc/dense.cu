@@ -408,10 +408,14 @@ std::string gemm_profile_table() {
 // Products with at most 16 columns (the solve sweeps: a box block times a few
 // right-hand sides) are latency-bound in 64x64 tiles: one tile column, the K
 // loop of a whole chain in a handful of CTAs.  Here every (32-row block,
-// problem, 256-column K chunk) is its own CTA writing a partial sum; a second
-// kernel adds each output's partials in a fixed order (deterministic) and
-// applies alpha, beta.
-constexpr int SK_ROWS = 32, SK_KC = 256, SK_NR = 16;
+// problem, K chunk of up to 512) is its own CTA: it stages its chunk of B in
+// shared memory, its 8 warps split the chunk's depths (lane = row, so the
+// loads of A are 512 contiguous bytes per warp, several in flight), and the
+// warps' sums are added in a fixed order.  An output that one CTA covers
+// (depth up to 512, no chain) is written with alpha and beta by that CTA;
+// otherwise the CTAs write partial sums and a second kernel adds each
+// output's partials in a fixed order (deterministic) and applies alpha, beta.
+constexpr int SK_ROWS = 32, SK_KC = 512, SK_NR = 16;
 struct SkItem {
   int prob, row0, k0, klen, slot;
 };
@@ -419,8 +423,12 @@ struct SkOut {
   int head, row0, s0, ns;
 };
 
+// NR: columns held per thread (8 or 16, at least the launch's widest problem)
+template <bool DIRECT, int NR>
 __global__ void __launch_bounds__(256) zskinny_partial_kernel(const GemmProblem* __restrict__ probs,
-                                                              const SkItem* __restrict__ items, zd* __restrict__ part) {
+                                                              const SkItem* __restrict__ items, zd* __restrict__ part,
+                                                              int nmax) {
+  extern __shared__ zd sk_b[];  // the item's chunk of B: depth kk, column r at sk_b[kk * nmax + r]
   __shared__ zd red[8][8][SK_ROWS];
   const SkItem it = items[blockIdx.x];
   const GemmProblem& P = probs[it.prob];
@@ -428,18 +436,24 @@ __global__ void __launch_bounds__(256) zskinny_partial_kernel(const GemmProblem*
   const int row = it.row0 + lane;
   const bool live = row < P.m;
   const int n = P.n;
-  zd acc[SK_NR];
+  for (int t = threadIdx.x; t < it.klen * n; t += blockDim.x) {
+    const int kk = t % it.klen, r = t / it.klen;  // consecutive threads: consecutive depths of one column
+    sk_b[kk * nmax + r] = P.B[(size_t)r * P.ldb + it.k0 + kk];
+  }
+  __syncthreads();
+  zd acc[NR];
 #pragma unroll
-  for (int r = 0; r < SK_NR; ++r) acc[r] = zmk(0, 0);
-  const zd* A = P.A + (live ? row : 0);
-  const int kend = it.k0 + it.klen;
-#pragma unroll 2
-  for (int k = it.k0 + w; k < kend; k += 8) {
-    const zd a = live ? A[(size_t)k * P.lda] : zmk(0, 0);
+  for (int r = 0; r < NR; ++r) acc[r] = zmk(0, 0);
+  const zd* A = P.A + (size_t)it.k0 * P.lda + (live ? row : 0);
+  // 8 depths per warp in flight: each is a 512-byte row segment of A
+#pragma unroll 8
+  for (int kk = w; kk < it.klen; kk += 8) {
+    const zd a = live ? A[(size_t)kk * P.lda] : zmk(0, 0);
+    const zd* bk = sk_b + kk * nmax;
 #pragma unroll
-    for (int r = 0; r < SK_NR; ++r)
+    for (int r = 0; r < NR; ++r)
       if (r < n) {
-        const zd b = __ldg(P.B + (size_t)r * P.ldb + k);
+        const zd b = bk[r];
         acc[r].x = fma(a.x, b.x, acc[r].x);
         acc[r].x = fma(-a.y, b.y, acc[r].x);
         acc[r].y = fma(a.x, b.y, acc[r].y);
@@ -448,7 +462,7 @@ __global__ void __launch_bounds__(256) zskinny_partial_kernel(const GemmProblem*
   }
   zd* out = part + (size_t)it.slot * SK_NR * SK_ROWS;
 #pragma unroll
-  for (int half = 0; half < 2; ++half) {
+  for (int half = 0; half < NR / 8; ++half) {
 #pragma unroll
     for (int r = 0; r < 8; ++r) red[w][r][lane] = acc[half * 8 + r];
     __syncthreads();
@@ -456,7 +470,17 @@ __global__ void __launch_bounds__(256) zskinny_partial_kernel(const GemmProblem*
     zd sum = red[0][r][l];
 #pragma unroll
     for (int q = 1; q < 8; ++q) sum = zadd(sum, red[q][r][l]);
-    out[(size_t)(half * 8 + r) * SK_ROWS + l] = sum;
+    if (DIRECT) {
+      const int c = half * 8 + r, rr = it.row0 + l;
+      if (c < n && rr < P.m) {
+        zd* cp = P.C + (size_t)c * P.ldc + rr;
+        zd v = zmul(P.alpha, sum);
+        if (!(P.beta.x == 0.0 && P.beta.y == 0.0)) v = zadd(v, zmul(P.beta, *cp));
+        *cp = v;
+      }
+    } else {
+      out[(size_t)(half * 8 + r) * SK_ROWS + l] = sum;
+    }
     __syncthreads();
   }
 }
@@ -512,11 +536,29 @@ static void zgemm_skinny_chained(aifmm_ctx* ctx, const std::vector<GemmProblem>&
     i += len;
   }
   if (outs.empty()) return;
-  DevBuf dp = upload(ctx, ps), di = upload(ctx, items), dout = upload(ctx, outs);
+  int nmax = 1;
+  bool direct = true;  // every output covered by one CTA
+  for (const GemmProblem& p : ps) nmax = std::max(nmax, p.n);
+  for (const SkOut& o : outs) direct = direct && o.ns == 1;
+  const size_t smem = sizeof(zd) * (size_t)SK_KC * nmax;
+  // one instantiation per (direct, columns per thread)
+  auto kernel = [&](bool d) -> void (*)(const GemmProblem*, const SkItem*, zd*, int) {
+    if (nmax <= 8) return d ? zskinny_partial_kernel<true, 8> : zskinny_partial_kernel<false, 8>;
+    return d ? zskinny_partial_kernel<true, 16> : zskinny_partial_kernel<false, 16>;
+  };
+  smem_attr_once((const void*)kernel(direct), ctx->device, (int)(sizeof(zd) * SK_KC * SK_NR));
+  DevBuf dp = upload(ctx, ps), di = upload(ctx, items);
+  if (direct) {
+    kernel(true)<<<(unsigned)items.size(), 256, smem, ctx->stream>>>(dp.as<GemmProblem>(), di.as<SkItem>(), nullptr,
+                                                                     nmax);
+    AIFMM_LAUNCHED();
+    return;
+  }
+  DevBuf dout = upload(ctx, outs);
   DevBuf part(ctx, sizeof(zd) * (size_t)std::max(slots, 1) * SK_NR * SK_ROWS);
   if (!items.empty()) {
-    zskinny_partial_kernel<<<(unsigned)items.size(), 256, 0, ctx->stream>>>(dp.as<GemmProblem>(), di.as<SkItem>(),
-                                                                            part.as<zd>());
+    kernel(false)<<<(unsigned)items.size(), 256, smem, ctx->stream>>>(dp.as<GemmProblem>(), di.as<SkItem>(),
+                                                                      part.as<zd>(), nmax);
     AIFMM_LAUNCHED();
   }
   zskinny_reduce_kernel<<<(unsigned)outs.size(), SK_ROWS * SK_NR, 0, ctx->stream>>>(dp.as<GemmProblem>(),

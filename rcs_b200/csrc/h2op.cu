@@ -306,10 +306,10 @@ void H2Operator::apply(const zd* x, int ldx, zd* y, int ldy, int nr) {
   AIFMM_REQUIRE(nr >= 1, AIFMM_EINVAL, "no columns");
   AIFMM_REQUIRE(ldx >= N && ldy >= N, AIFMM_EINVAL, "leading dimension below N");
   AIFMM_CUDA(cudaSetDevice(ctx->device));
-  const long before = launch_count();
+  const long before = thread_launch_count();
   for (int c0 = 0; c0 < nr; c0 += SKINNY_MAXNR)
     applyChunk(x + (size_t)c0 * ldx, ldx, y + (size_t)c0 * ldy, ldy, std::min(SKINNY_MAXNR, nr - c0));
-  launchesPerApply = launch_count() - before;
+  launchesPerApply = thread_launch_count() - before;
 }
 
 // Upward P2M, M2L per level, downward L2P, leaf L2P + near field, all in tree order.

@@ -655,11 +655,15 @@ __device__ void rrqr_p2_apply_col(const RRQRProblem& P, int j, int q, int lane) 
   const zd* h = P.H + (size_t)P.istate[7] * m;
   zd* y = P.R + (size_t)P.perm[q] * m;
   zd a = zmk(0, 0);
+  // unrolled so that several loads of h and y are in flight per lane (the
+  // accumulation order of each lane is unchanged)
+#pragma unroll 4
   for (int i = j + lane; i < m; i += 32) a = zadd(a, zcmul(h[i], y[i]));
   for (int o = 16; o > 0; o >>= 1) {
     a.x += __shfl_xor_sync(0xffffffff, a.x, o);
     a.y += __shfl_xor_sync(0xffffffff, a.y, o);
   }
+#pragma unroll 4
   for (int i = j + lane; i < m; i += 32) y[i] = zsub(y[i], zmul(h[i], a));
   __syncwarp();
   if (q == j) {

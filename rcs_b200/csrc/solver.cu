@@ -1411,8 +1411,10 @@ void Solver::rhsEliminateX(int j, int k) {  // T:3613-3653, :3795-3886
   DBox& B = tree[j][k];
   if (B.P2P[k].size() != 0) {
     const DMat y = ops.mul(B.invP2P, OP_N, B.particle_rhs, OP_N);
-    B.local_rhs = ops.mul(B.P2M, OP_N, y, OP_N, MONE);
+    // local_rhs = -P2M y rides in the same launch as the neighbour updates
+    B.local_rhs = ops.alloc(B.P2M.r, nrhs_);
     GemmBatch g;
+    g.add(B.local_rhs, B.P2M, OP_N, y, OP_N, MONE, ZERO);
     for (int nn : B.NB) {
       if (nn == k) continue;
       DBox& Bn = tree[j][nn];
@@ -1569,7 +1571,7 @@ void Solver::capturePlan(int nrhs) {
   pl->hold->ctx = ctx;
   if (!ctx->sideStream) AIFMM_CUDA(cudaStreamCreateWithFlags(&ctx->sideStream, cudaStreamNonBlocking));
   AIFMM_CUDA(cudaStreamSynchronize(ctx->stream));
-  const long l0 = launch_count();
+  const long l0 = thread_launch_count();
   AIFMM_CUDA(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
   ctx->capture = pl->hold;
   try {
@@ -1581,12 +1583,12 @@ void Solver::capturePlan(int nrhs) {
     cudaStreamEndCapture(ctx->stream, &g);
     if (g) cudaGraphDestroy(g);
     cudaGetLastError();
-    count_launch(l0 - launch_count());
+    count_launch(l0 - thread_launch_count());
     throw;
   }
   ctx->capture.reset();
   const cudaError_t e = cudaStreamEndCapture(ctx->stream, &pl->graph);
-  pl->launches = launch_count() - l0;
+  pl->launches = thread_launch_count() - l0;
   count_launch(-pl->launches);
   AIFMM_CUDA(e);
   AIFMM_CUDA(cudaGraphInstantiate(&pl->exec, pl->graph, 0));

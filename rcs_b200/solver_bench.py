@@ -4,7 +4,7 @@
                                     [--levels 3] [--tol-pow 5] [--fillin-tol 7]
                                     [--precision 0-4] [--drop-pow 0] [--op-tol 10] [--nrhs 8]
                                     [--gmres 1e-6] [--profile-ops] [--profile-host] [--profile-gemm]
-                                    [--profiler-range]
+                                    [--profiler-range] [--profile-solve]
 
 Builds the EFIE operator of an icosphere (subdivision --sub), assembles the
 AIFMM solver and, when --gmres is given, the FP64 H^2 forward operator; then
@@ -16,7 +16,9 @@ per-operation accounting on (every accounted operation then synchronises) and
 prints its table.  --profiler-range brackets the timed factorization and
 solve with cudaProfilerStart/Stop, so that a kernel profiler run with
 capture from start off (ncu --profile-from-start off) records exactly their
-launches.
+launches.  --profile-solve times one direct solve issued launch by launch and
+one replayed from the captured CUDA graph, then runs one more launch-by-launch
+solve between cudaProfilerStart/Stop (for a launch list of the sweep).
 """
 from __future__ import annotations
 
@@ -49,6 +51,8 @@ def main():
                     help="time the factorization with host-only accounting (no extra synchronisation)")
     ap.add_argument("--profiler-range", action="store_true",
                     help="cudaProfilerStart/Stop around the timed factorization and solve")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="time eager and graph-replayed direct solves; profiler range around one eager solve")
     a = ap.parse_args()
     from . import mesh as M
     from .kernel import EFIEMatrix
@@ -104,6 +108,25 @@ def main():
     if a.profiler_range:
         torch.cuda.synchronize()
         torch.cuda.profiler.stop()
+    if a.profile_solve:
+        import torch
+        times = {}
+        for mode in (False, True):
+            S.set_graph_solve(mode)
+            S.solve(B)  # warm-up (the graph mode captures here)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            S.solve(B)
+            times["graph" if mode else "eager"] = time.perf_counter() - t0
+        S.set_graph_solve(False)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.start()
+        S.solve(B)
+        torch.cuda.synchronize()
+        torch.cuda.profiler.stop()
+        S.set_graph_solve(True)
+        print(f"# direct solve of {a.nrhs} right-hand sides: launch by launch {times['eager']:.4f} s, "
+              f"graph replay {times['graph']:.4f} s")
     info = S.info()
     if a.precision == 5:
         for line in K.ctx.tune_report():

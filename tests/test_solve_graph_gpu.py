@@ -51,7 +51,10 @@ def test_graph_solve_matches_launch_by_launch(K, precision):
     S.set_graph_solve(False)
     E3c = S.solve(B3)
     assert np.array_equal(G3c, E3c)
-    assert np.linalg.norm(G3c - E3) <= 1e-8 * np.linalg.norm(E3)
+    # the refactorization starts from a copy of the assembled blocks, and the
+    # first factorization after assembly rounds differently (about 1e-15);
+    # split TF32 amplifies that to FP32-level differences
+    assert np.linalg.norm(G3c - E3) <= (1e-8 if precision == 0 else 1e-4) * np.linalg.norm(E3)
     S.close()
 
 
