@@ -5,7 +5,7 @@
 // every size; each stream-ordered pool call for a large block costs tens of
 // microseconds to milliseconds of host time.  The arena carves such blocks
 // out of chunks it keeps -- 64 MB at first, each new chunk as large as all
-// earlier ones together up to 1 GB (so a small body's context, one of a
+// earlier ones together up to 512 MB (so a small body's context, one of a
 // batch of dozens, holds little), or one request's size when larger: a free
 // block is found by size in a multimap, split, and merged with its free
 // neighbours of the same chunk when released.  Every use of context memory
@@ -27,7 +27,7 @@ namespace aifmm {
 class Arena {
  public:
   static constexpr size_t kAlign = 512;
-  static constexpr size_t kChunk = (size_t)1 << 30;       // largest growth step
+  static constexpr size_t kChunk = (size_t)512 << 20;     // largest growth step
   static constexpr size_t kFirstChunk = (size_t)64 << 20;  // first growth step
   static constexpr size_t kMinSize = (size_t)256 << 10;
 
