@@ -68,3 +68,42 @@ def test_noalloc_rrqr_rejects_oversized_problem():
         _lib.check(_lib.lib().aifmm_rrqr_noalloc(C.c_void_p(Ad.data_ptr()), m, n, 10, 8, 8, 1.0, 5, 0,
                                                  C.c_void_p(Qd.data_ptr()), C.c_void_p(rk.data_ptr()),
                                                  C.c_void_p(mp.data_ptr()), None))
+
+
+def test_noalloc_rrqr_captures_in_a_cuda_graph():
+    """The property the entry point exists for: after a first call, a call
+    allocates nothing and can be captured in a CUDA graph; replays give the
+    eager call's results bit for bit and leave the input untouched."""
+    import torch
+    from rcs_b200 import _lib
+    seed, m, r0, nf, frank, tp1, tp2, fill, pivot = (11, 60, 10, 30, 8, 8, 10, 5, 10.0)
+    A = _case(seed, m, r0, nf, frank)
+    Q_ref, mp_ref, _ = _noalloc(A, tp1, tp2, r0, pivot, fill)  # the first call looks up the scratch array
+    n = A.shape[1]
+    Ad = torch.from_numpy(np.ascontiguousarray(A.T)).cuda()
+    Qd = torch.zeros((min(m, n), m), dtype=torch.complex128, device="cuda")
+    rk = torch.zeros(1, dtype=torch.int32, device="cuda")
+    mp = torch.zeros(1, dtype=torch.float64, device="cuda")
+
+    def call(stream):
+        _lib.check(_lib.lib().aifmm_rrqr_noalloc(C.c_void_p(Ad.data_ptr()), m, n, r0, tp1, tp2, float(pivot), fill,
+                                                 0, C.c_void_p(Qd.data_ptr()), C.c_void_p(rk.data_ptr()),
+                                                 C.c_void_p(mp.data_ptr()), C.c_void_p(stream)))
+
+    torch.cuda.synchronize()
+    free0 = torch.cuda.mem_get_info()[0]
+    call(torch.cuda.current_stream().cuda_stream)  # an eager call after the first: no device allocation
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    Qd.zero_()
+    rk.zero_()
+    mp.zero_()
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        call(torch.cuda.current_stream().cuda_stream)
+    for _ in range(2):
+        g.replay()
+        torch.cuda.synchronize()
+        r = int(rk.item())
+        assert np.array_equal(Qd.cpu().numpy()[:r].T, Q_ref) and float(mp.item()) == mp_ref
+    assert np.array_equal(Ad.cpu().numpy().T, A)
