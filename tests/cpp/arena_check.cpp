@@ -4,10 +4,13 @@
 // that an emptied arena hands every chunk back whole; chunks that happen to be
 // adjacent in the address space are never merged; chunks handed back while
 // other chunks still hold ranges contain no live range and are never handed
-// out again.  Exit 0 and "OK" on success.
+// out again.  The growth policy: 64 MB first, then as much as the arena holds,
+// at most 512 MB a step, and one request's size when it is larger.  Exit 0
+// and "OK" on success.
 #include <cstdio>
 #include <map>
 #include <random>
+#include <vector>
 
 #include "../../rcs_b200/csrc/arena.cuh"
 
@@ -90,6 +93,23 @@ int main() {
   CHECK(a.freeRanges() == nChunks);  // every chunk merged back into one range
   auto freed = a.takeFreeChunks();
   CHECK(freed.size() == nChunks && a.chunks().empty());
+  {  // growth steps of a fresh arena under small requests, then one larger than a step
+    std::vector<size_t> steps;
+    uint64_t nb = (uint64_t)1 << 44;
+    Arena g([&](size_t bytes) -> uint64_t {
+      steps.push_back(bytes);
+      const uint64_t base = nb;
+      nb += bytes;
+      return base;
+    });
+    const size_t MB = (size_t)1 << 20;
+    for (int t = 0; t < 3000; ++t) CHECK(g.alloc(MB) != 0);  // 3000 MB in 1 MB ranges
+    const size_t want[] = {64 * MB, 64 * MB, 128 * MB, 256 * MB, 512 * MB, 512 * MB, 512 * MB, 512 * MB, 512 * MB};
+    CHECK(steps.size() == sizeof(want) / sizeof(want[0]));
+    for (size_t i = 0; i < steps.size() && i < sizeof(want) / sizeof(want[0]); ++i) CHECK(steps[i] == want[i]);
+    CHECK(g.alloc(700 * MB) != 0);  // larger than a step: a chunk of its own size
+    CHECK(steps.back() == 700 * MB);
+  }
   if (fails == 0) std::printf("OK %zu chunks\n", nChunks);
   return fails ? 1 : 0;
 }

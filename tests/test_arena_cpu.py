@@ -1,7 +1,8 @@
 """The device sub-allocator's bookkeeping (rcs_b200/csrc/arena.cuh) under a
 randomised sequence of 60,000 allocations and releases with fake chunk
 addresses: ranges inside one chunk, aligned, disjoint; an emptied arena hands
-every chunk back whole; adjacent chunks never merge (tests/cpp/arena_check.cpp)."""
+every chunk back whole; adjacent chunks never merge; chunks grow 64 MB first,
+then geometrically up to 512 MB a step (tests/cpp/arena_check.cpp)."""
 import os
 import shutil
 import subprocess
