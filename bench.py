@@ -46,7 +46,7 @@ CONFIGS = {
                     "fill-ins under 1e-1 of their M2L block dropped) as the preconditioner of FP64 FGMRES(30) to "
                     "1e-6 on an ACA-1e-9 H2 operator"),
     "c2": dict(N=81920, kind="es", sub=6, radius=1.0, leaf=128, tol_pow=5, fillin_tol=7, nrhs=33, levels=0,
-               op_tol=10, gmres=1e-8, precision=4,
+               op_tol=10, gmres=1e-8, precision=4, drop_pow=1,
                desc="Electrostatics unit sphere, 81,920 flat triangles (piecewise-constant charge, collocation at "
                     "centroids), leaf 128, ACA 1e-5, RRQR 1e-7, 32 seeded N(0,1) potentials + the 1 V conductor "
                     "RHS, mixed factorization (split-TF32 tcgen05 GEMMs, FP32-class) as the preconditioner of FP64 "
